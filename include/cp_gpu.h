@@ -1,0 +1,228 @@
+/*
+ * cp_gpu.h -- C ABI of the B200 crystal-plasticity quadrature-point library.
+ *
+ * The library replaces, for a batch of quadrature points (qps) resident on one
+ * GPU, the per-qp hot path of PRISMS-Plasticity's crystalPlasticity<dim> model:
+ *
+ *   calculatePlasticity(cellID, q, StiffnessCalFlag)
+ *       src/materialModels/crystalPlasticity/calculatePlasticity.cc:13-1022
+ *       (declared include/crystalPlasticity.h:77)
+ *   inactive_slip_removal(...)       .../inactiveSlipRemoval.cc:4-124
+ *   the inline algorithmic tangent   .../calculatePlasticity.cc:473-940
+ *       (include/crystalPlasticity.h:48 declares tangent_modulus, never defined)
+ *   getElementalValues(...) qp loop   .../getElementalValues.cc:127-163
+ *       (pure virtual in include/ellipticBVP.h:130, override crystalPlasticity.h:78)
+ *   reorient()                       .../reorient.cc:4-98
+ *   history commit _iter -> _conv    .../updateAfterIncrement.cc:287-305
+ *   volume averages                  .../updateAfterIncrement.cc:119-126,218-235,710-722
+ *
+ * Conventions
+ *   - Every function returns an int status: CP_OK (0) or a negative CP_E* code;
+ *     cp_last_error() gives a one-line message for the handle's last failure.
+ *   - Pointers named h_* are host pointers, borrowed for the duration of the
+ *     call (they may be pageable; the library stages them through its own
+ *     pinned buffers).  Pointers named d_* are device pointers on the handle's
+ *     GPU; those calls are asynchronous on the handle's stream unless noted.
+ *   - 3x3 tensors are row-major (A[i][j] at 3*i+j); a batch of tensors is
+ *     qp-major: qp k's tensor starts at 9*k.  dP/dF is dPdF[m][n][o][p] at
+ *     81*k + 27*m + 9*n + 3*o + p (the reference's Tensor<4,3> dP_dF).
+ *   - Voigt order everywhere is (11,22,33,23,13,12) as in vecform/matform
+ *     (matrixOperations.cc:133-163).
+ *   - One CUDA stream per handle; no global mutable state; calls on different
+ *     handles may come from different host threads.  A handle is not
+ *     re-entrant (like the reference class, which keeps scratch in members).
+ *   - There is no CPU fallback: if the CUDA kernels cannot be launched the
+ *     call fails with CP_E_CUDA.
+ */
+#ifndef CP_GPU_H
+#define CP_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CP_MAX_SYSTEMS 64  /* slip + twin systems per lattice, dummy twin included */
+#define CP_MAX_LATTICES 8  /* phases per handle (the reference supports up to 4) */
+
+/* return codes */
+#define CP_OK 0
+#define CP_E_ARG (-1)      /* invalid argument / size */
+#define CP_E_STATE (-2)    /* call out of order (e.g. cp_update before cp_bind_qps) */
+#define CP_E_CUDA (-3)     /* CUDA runtime error */
+#define CP_E_NOMEM (-4)    /* device or pinned allocation failed */
+#define CP_E_UNSUPPORTED (-5)
+
+/* per-qp status bits written by cp_update / cp_assemble (0 = clean) */
+#define CP_QP_NONFINITE 1       /* a NaN/Inf reached P, T or dP/dF */
+#define CP_QP_SINGULAR 2        /* a zero pivot in an active-set or tangent solve */
+#define CP_QP_ACTIVE_OVERFLOW 4 /* potentially active set larger than the kernel's tile */
+#define CP_QP_SERIES_CAP 8      /* exp / Gateaux series hit its term cap */
+#define CP_QP_SLIP_SEARCH_CAP 16 /* informational: slip-search cap reached (reference truncates silently, calculatePlasticity.cc:155-158) */
+
+/*
+ * One lattice (phase).  Field names follow userInputParameters
+ * (src/userInputParameters/userInputParameters.cc:255-323) and the per-phase
+ * members loaded by multiphaseInit (multiphaseInit.cc:4-67).
+ * Systems 0..n_slip-1 are slip systems, n_slip..n_slip+n_twin-1 twin systems.
+ * With twinning disabled the reference appends ONE dummy twin system
+ * (init.cc:37-41,178-185; userInputParameters.cc:303-311): callers build it
+ * with cp_material_add_dummy_twin().
+ */
+typedef struct cp_material_t {
+    int32_t n_slip;               /* numSlipSystems */
+    int32_t n_twin;               /* numTwinSystems (1 = the dummy when twinning is off) */
+    int32_t twinning_enabled;     /* enableTwinning: twin reorientation branch */
+    int32_t reserved;
+    double elastic_stiffness[36]; /* 6x6 Voigt, row-major: "Elastic Stiffness row 1..6" */
+    double slip_normal[CP_MAX_SYSTEMS * 3];    /* n_alpha, unit length */
+    double slip_direction[CP_MAX_SYSTEMS * 3]; /* m_alpha, unit length */
+    double latent_hardening[CP_MAX_SYSTEMS * CP_MAX_SYSTEMS]; /* q[a][b] at a*CP_MAX_SYSTEMS+b */
+    double initial_slip_resistance[CP_MAX_SYSTEMS];   /* s0 */
+    double initial_hardening_modulus[CP_MAX_SYSTEMS]; /* h0 */
+    double saturation_stress[CP_MAX_SYSTEMS];         /* s_s */
+    double power_law_exponent[CP_MAX_SYSTEMS];        /* a */
+    double kinematic_c1[CP_MAX_SYSTEMS];              /* C_1 (0 when kinematic hardening is off) */
+    double kinematic_c2[CP_MAX_SYSTEMS];              /* C_2 */
+    double twin_threshold_fraction;  /* twinThresholdFraction */
+    double twin_saturation_factor;   /* twinSaturationFactor */
+    double twin_shear;               /* twinShear ("Characteristic Twin Shear") */
+} cp_material_t;
+
+/* Numerical options (userInputParameters.cc:320-323) and execution knobs. */
+typedef struct cp_options_t {
+    double stress_tolerance;            /* modelStressTolerance ("Stress Tolerance") */
+    int32_t max_slip_search_iterations; /* modelMaxSlipSearchIterations */
+    int32_t max_solver_iterations;      /* modelMaxSolverIterations */
+    int32_t enable_multiphase;          /* F_T rule, calculatePlasticity.cc:970-980 */
+    int32_t device;                     /* CUDA device ordinal */
+    int32_t block_size;                 /* threads per block for the qp kernels (0 = autotuned) */
+    int32_t use_graphs;                 /* capture repeated launches in CUDA graphs (1) */
+} cp_options_t;
+
+typedef struct cp_handle cp_handle;
+
+/* Fill *opts with the reference defaults (tol 1e-9, caps 1/1, device 0). */
+int cp_options_default(cp_options_t* opts);
+
+/* Append the reference's dummy twin system to a twinning-disabled lattice:
+ * CRSS 10e14, h0 1, a 0, s_s 10e15, n=(1,0,0), m=(0,1,0), zero q row/col
+ * (userInputParameters.cc:303-311, init.cc:51-65,178-185). */
+int cp_material_add_dummy_twin(cp_material_t* mat);
+
+/*
+ * Create a handle for n_lattices phases on opts->device.
+ * Replaces the constructor + multiphaseInit: all per-lattice constants go to
+ * the device once instead of being reloaded on every qp call
+ * (multiphaseInit.cc:4-67 runs at calculatePlasticity.cc:17).
+ */
+int cp_create(const cp_material_t* lattices, int32_t n_lattices,
+              const cp_options_t* opts, cp_handle** out);
+void cp_destroy(cp_handle* h);
+const char* cp_last_error(const cp_handle* h);
+
+/*
+ * Allocate the resident per-qp history (init.cc:198-330): Fp=Fe=I, s=s0,
+ * W=0, twin/slip fractions 0, twin flag 0, rot=rotnew=rodrigues.
+ * lattice_id[k] in [0, n_lattices); h_rodrigues is 3*n_qp (orientation of qp k).
+ * Internally qps are grouped by lattice; all qp-indexed arrays of the API stay
+ * in the caller's order.
+ */
+int cp_bind_qps(cp_handle* h, int64_t n_qp, const int32_t* h_lattice_id,
+                const double* h_rodrigues);
+int64_t cp_num_qps(const cp_handle* h);
+
+/*
+ * Batched calculatePlasticity(cellID, q, stiffness_flag) for every bound qp.
+ * h_F: 9*n_qp deformation gradients.  Outputs (may be NULL when unwanted):
+ * h_P (first Piola, 9*n_qp), h_T (Cauchy, 9*n_qp), h_dPdF (81*n_qp, only
+ * written when stiffness_flag == 1), h_status (n_qp status bits).
+ * F_e / F_r are the previous increment's volume-averaged twin quantities
+ * (updateAfterIncrement.cc:719-720) used by the twin-reorientation threshold.
+ * Synchronous: returns when the outputs are in host memory.
+ */
+int cp_update(cp_handle* h, const double* h_F, int32_t stiffness_flag,
+              double F_e, double F_r, double* h_P, double* h_T, double* h_dPdF,
+              int32_t* h_status);
+
+/* Same on device buffers, asynchronous on the handle's stream. */
+int cp_update_device(cp_handle* h, const double* d_F, int32_t stiffness_flag,
+                     double F_e, double F_r, double* d_P, double* d_T,
+                     double* d_dPdF, int32_t* d_status);
+
+/*
+ * Per-qp work statistics of the last cp_update / cp_assemble (device buffer
+ * kept by the handle), copied to h_stats as 8 int32 per qp:
+ *   [0] potentially active systems p0, [1] final active systems p,
+ *   [2] active-set removal rounds, [3] exp series terms e,
+ *   [4] Gateaux series terms c (count3), [5] slip-search passes,
+ *   [6] lattice id, [7] reserved.
+ */
+int cp_get_stats(cp_handle* h, int32_t* h_stats);
+
+/*
+ * Element mesh for the fused assembly: n_cells hexahedral Q1 cells with 8
+ * Gauss points each; qp k = 8*cell + q must be the bound qp of that point.
+ * h_grad_N: shape-function gradients, [cell][q][node a][3] (8*8*3 doubles per
+ * cell), or one cell's worth shared by all cells when uniform != 0.
+ * h_JxW: [cell][q] (or [q] when uniform).  Local dof d = 3*a + c is component
+ * c of node a (FESystem<FE_Q<1>,3> ordering).
+ */
+int cp_bind_mesh(cp_handle* h, int64_t n_cells, const double* h_grad_N,
+                 const double* h_JxW, int32_t uniform);
+
+/*
+ * Batched getElementalValues (getElementalValues.cc:127-163): for every cell,
+ * F = I + sum_d U_d grad N_d at each qp, calculatePlasticity(...,1), then
+ * Re[d] -= gradN_d . P . JxW and Ke[d1][d2] += gradN_d1 . dPdF . gradN_d2 JxW.
+ * h_U_local: 24*n_cells; outputs h_Ke 576*n_cells (row-major 24x24, not
+ * symmetric), h_Re 24*n_cells.
+ */
+int cp_assemble(cp_handle* h, const double* h_U_local, double F_e, double F_r,
+                double* h_Ke, double* h_Re, int32_t* h_status);
+int cp_assemble_device(cp_handle* h, const double* d_U_local, double F_e,
+                       double F_r, double* d_Ke, double* d_Re, int32_t* d_status);
+
+/*
+ * Volume averages over the bound mesh after a post-pass update, as
+ * updateAfterIncrement.cc:119-126,218-235,710-722 accumulates them, using the
+ * F of the last cp_update (E = (F^T F - I)/2) and its Cauchy stress.
+ * out[0..8] strain E (3x3 row-major), out[9..17] stress T, out[18] F_r
+ * (twin fraction), out[19] F_e (twinned volume), out[20] F_s (slip), out[21]
+ * volume.  Requires cp_bind_mesh (for JxW).
+ */
+int cp_averages(cp_handle* h, double out[22]);
+
+/* reorient() (reorient.cc:4-98) on all qps: updates rotnew_conv. */
+int cp_reorient(cp_handle* h);
+
+/* Commit the increment: *_conv = *_iter (updateAfterIncrement.cc:287-305). */
+int cp_commit(cp_handle* h);
+
+/* History fields for cp_get_state / cp_set_state.  Per-qp widths: */
+#define CP_FIELD_FP_CONV 0       /* 9 */
+#define CP_FIELD_FE_CONV 1       /* 9 */
+#define CP_FIELD_S_CONV 2        /* n_T of the qp's lattice, padded to the handle's max n_T */
+#define CP_FIELD_W_CONV 3        /* same */
+#define CP_FIELD_ROT_CONV 4      /* 3 */
+#define CP_FIELD_ROTNEW_CONV 5   /* 3 */
+#define CP_FIELD_TWINFRAC_CONV 6 /* n_twin, padded to the handle's max n_twin */
+#define CP_FIELD_SLIPFRAC_CONV 7 /* n_slip, padded to the handle's max n_slip */
+#define CP_FIELD_TWIN_CONV 8     /* 1 (0.0 or 1.0) */
+#define CP_FIELD_ITER_OFFSET 16  /* add to get the *_iter field */
+#define CP_FIELD_FP_ITER (CP_FIELD_ITER_OFFSET + CP_FIELD_FP_CONV)
+
+/* Width (doubles per qp) of a field in cp_get_state/cp_set_state. */
+int32_t cp_field_width(const cp_handle* h, int32_t field);
+/* Copy a history field to/from host (h_buf: width*n_qp doubles, caller order). */
+int cp_get_state(cp_handle* h, int32_t field, double* h_buf);
+int cp_set_state(cp_handle* h, int32_t field, const double* h_buf);
+
+/* Wait for all work queued on the handle's stream. */
+int cp_synchronize(cp_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CP_GPU_H */

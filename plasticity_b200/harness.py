@@ -1,0 +1,246 @@
+"""Host Newton harness: a minimal restatement of the reference's ellipticBVP
+driver around the qp hot path.
+
+It plays the part of the deal.II caller of the C ABI.  Reference pieces it
+restates (paths under src/):
+
+* mesh: subdivided unit cube refined ``r`` times -> n x n x n Q1 hexahedra
+  (ellipticBVP/mesh.cc:32,101), QGauss(2) -> 8 qps per cell, FESystem dof
+  ordering (local dof d = 3*vertex + component, vertices lexicographic);
+* Dirichlet BCs from a (face, dof, total displacement) table
+  (ellipticBVP/boundaryConditions.cc:79-118): the value is applied at Newton
+  iteration 0 only, 0 afterwards (boundaryConditions.cc:485-490), with
+  deluConstraint = totalU / totalIncrements (ellipticBVP/init.cc:326-343);
+* exactly ``max_newton`` assemble+solve passes per increment, no convergence
+  test (ellipticBVP/solveNonLinearSystem.cc:14-81);
+* the increment commit of updateAfterIncrement.cc: post-pass update with
+  StiffnessCalFlag 0 (:105), volume averages (:119-126,218-235,710-722),
+  reorient (:291), *_iter -> *_conv (:298-305), and the stressstrain.txt
+  row (:733-771).
+
+The Newton-step linear system is solved directly (sparse LU) on the host; the
+reference uses PETSc BiCG + Jacobi to 1e-10 relative residual
+(ellipticBVP/solveLinearSystem.cc:14-16).
+
+The backend is any object with the CpHandle method set (the GPU library, or
+in tests the CPU oracle).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+GAUSS = (0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0))
+
+
+def q1_reference_gradients():
+    """d N_a / d xi at the 8 Gauss points of the unit reference cube:
+    array [q][a][3], q and a lexicographic (x fastest)."""
+    g = np.zeros((8, 8, 3))
+    for q in range(8):
+        xi = (GAUSS[q & 1], GAUSS[(q >> 1) & 1], GAUSS[(q >> 2) & 1])
+        for a in range(8):
+            bits = (a & 1, (a >> 1) & 1, (a >> 2) & 1)
+            f = [xi[d] if bits[d] else 1.0 - xi[d] for d in range(3)]
+            df = [1.0 if bits[d] else -1.0 for d in range(3)]
+            g[q, a, 0] = df[0] * f[1] * f[2]
+            g[q, a, 1] = f[0] * df[1] * f[2]
+            g[q, a, 2] = f[0] * f[1] * df[2]
+    return g
+
+
+@dataclasses.dataclass
+class StructuredMesh:
+    """n[0] x n[1] x n[2] uniform Q1 cells on [0,1]^3."""
+
+    n: tuple
+
+    def __post_init__(self):
+        nx, ny, nz = self.n
+        self.h = np.array([1.0 / nx, 1.0 / ny, 1.0 / nz])
+        self.n_nodes = (nx + 1) * (ny + 1) * (nz + 1)
+        self.n_dofs = 3 * self.n_nodes
+        self.n_cells = nx * ny * nz
+        ix, iy, iz = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+        node_id = lambda i, j, k: i + (nx + 1) * (j + (ny + 1) * k)
+        self.node_xyz = np.zeros((self.n_nodes, 3))
+        nid = node_id(ix, iy, iz)
+        self.node_xyz[nid.ravel(), 0] = ix.ravel() * self.h[0]
+        self.node_xyz[nid.ravel(), 1] = iy.ravel() * self.h[1]
+        self.node_xyz[nid.ravel(), 2] = iz.ravel() * self.h[2]
+        cells = []
+        for k in range(nz):
+            for j in range(ny):
+                for i in range(nx):
+                    cells.append([node_id(i + (a & 1), j + ((a >> 1) & 1), k + ((a >> 2) & 1)) for a in range(8)])
+        self.cell_nodes = np.array(cells, dtype=np.int64)
+        self.cell_dofs = (3 * self.cell_nodes[:, :, None] + np.arange(3)).reshape(self.n_cells, 24)
+        gref = q1_reference_gradients()
+        self.grad_N = gref / self.h  # uniform mesh: [q][a][3]
+        self.JxW = np.full(8, np.prod(self.h) / 8.0)
+        self._build_pattern()
+
+    def cell_centres(self):
+        return self.node_xyz[self.cell_nodes].mean(axis=1)
+
+    def _build_pattern(self):
+        rows = np.repeat(self.cell_dofs, 24, axis=1).ravel()
+        cols = np.tile(self.cell_dofs, (1, 24)).ravel()
+        lin = rows * self.n_dofs + cols
+        uniq, inv = np.unique(lin, return_inverse=True)
+        self._pos = inv
+        self._nnz = len(uniq)
+        r = uniq // self.n_dofs
+        c = uniq % self.n_dofs
+        self._indptr = np.searchsorted(r, np.arange(self.n_dofs + 1))
+        self._indices = c.astype(np.int32)
+        self._rows = r
+
+    def assemble_matrix(self, Ke):
+        data = np.bincount(self._pos, weights=np.asarray(Ke).ravel(), minlength=self._nnz)
+        return sp.csr_matrix((data, self._indices, self._indptr), shape=(self.n_dofs, self.n_dofs))
+
+    def assemble_vector(self, Re):
+        return np.bincount(self.cell_dofs.ravel(), weights=np.asarray(Re).ravel(), minlength=self.n_dofs)
+
+    def deformation_gradients(self, u):
+        """F = I + sum_d U_d grad N_d at every qp (getElementalValues.cc:129-138);
+        returns [cell*8 + q][9]."""
+        Ul = u[self.cell_dofs].reshape(self.n_cells, 8, 3)  # [cell][a][comp]
+        F = np.einsum("cai,qaj->cqij", Ul, self.grad_N)
+        F += np.eye(3)
+        return F.reshape(-1, 9)
+
+
+def face_nodes(mesh: StructuredMesh, face: int, eps: float = 1e-5):
+    """Faces 1..6 = x=0, x=1, y=0, y=1, z=0, z=1 (boundaryConditions.cc:84-111)."""
+    axis = (face - 1) // 2
+    x = mesh.node_xyz[:, axis]
+    return np.nonzero(x <= eps)[0] if face % 2 == 1 else np.nonzero(x >= 1.0 - eps)[0]
+
+
+def dirichlet_increments(mesh: StructuredMesh, bc_table, n_increments: int):
+    """Constrained dofs and their per-increment values.  A node on several
+    constrained faces takes the value of the lowest face id, as the early
+    return in setBoundaryValues does (boundaryConditions.cc:79-113)."""
+    constrained = {}
+    rows = sorted([(int(f), int(d), float(u)) for f, d, u in bc_table])
+    for face in range(1, 7):
+        for f, dof, total in rows:
+            if f != face:
+                continue
+            for nd in face_nodes(mesh, face):
+                gd = 3 * nd + (dof - 1)
+                if gd not in constrained:
+                    constrained[gd] = total / n_increments
+    dofs = np.array(sorted(constrained), dtype=np.int64)
+    vals = np.array([constrained[d] for d in dofs])
+    return dofs, vals
+
+
+def von_mises_rows(rows):
+    """run_compile_tests.py:45-48 on stressstrain rows."""
+    r = np.asarray(rows)
+    e = np.sqrt(0.5 * ((r[:, 0] - r[:, 1]) ** 2 + (r[:, 1] - r[:, 2]) ** 2 + (r[:, 2] - r[:, 0]) ** 2
+                       + 6 * (r[:, 3] ** 2 + r[:, 4] ** 2 + r[:, 5] ** 2)))
+    s = np.sqrt(0.5 * ((r[:, 6] - r[:, 7]) ** 2 + (r[:, 7] - r[:, 8]) ** 2 + (r[:, 8] - r[:, 6]) ** 2
+                       + 6 * (r[:, 9] ** 2 + r[:, 10] ** 2 + r[:, 11] ** 2)))
+    return e, s
+
+
+def golden_errors(new_rows, old_rows, check_rows):
+    """The reference's pass criterion (run_compile_tests.py:55-60): max relative
+    error of von Mises strain, von Mises stress and SlipTotal over the first
+    ``check_rows`` rows, nan -> 0 and inf -> max float as np.nan_to_num does."""
+    n = min(check_rows, len(new_rows), len(old_rows))
+    oe, os_ = von_mises_rows(old_rows[:n])
+    ne, ns = von_mises_rows(new_rows[:n])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        err = lambda a, b: float(np.max(np.nan_to_num(np.abs((a - b) / a))))
+        return {"strain": err(oe, ne), "stress": err(os_, ns),
+                "slip": err(np.asarray(old_rows)[:n, 14], np.asarray(new_rows)[:n, 14]),
+                "twin": err(np.asarray(old_rows)[:n, 13], np.asarray(new_rows)[:n, 13]), "rows": n}
+
+
+class NewtonHarness:
+    """Fixed-iteration Newton loop over a structured Q1 mesh."""
+
+    def __init__(self, backend, mesh: StructuredMesh, bc_table, n_increments: int, max_newton: int = 4,
+                 multiphase: bool = False):
+        self.be = backend
+        self.mesh = mesh
+        self.n_increments = n_increments
+        self.max_newton = max_newton
+        self.multiphase = multiphase
+        self.cdofs, self.cvals = dirichlet_increments(mesh, bc_table, n_increments)
+        self.u = np.zeros(mesh.n_dofs)
+        self.F_e = 0.0
+        self.F_r = 0.0
+        self.rows = []
+        mask = np.zeros(mesh.n_dofs, dtype=bool)
+        mask[self.cdofs] = True
+        self.cmask = mask
+        self._zero_entries = mask[mesh._rows] | mask[mesh._indices]
+        self._diag = None
+        backend.bind_mesh(mesh.n_cells, mesh.grad_N, mesh.JxW, True)
+
+    def _solve(self, K, R, duc):
+        """K du = R with du[c] = duc (constraints condensed as deal.II's
+        distribute_local_to_global with inhomogeneities does)."""
+        du_full = np.zeros(self.mesh.n_dofs)
+        du_full[self.cdofs] = duc
+        rhs = R - K @ du_full
+        K = K.copy()
+        K.data[self._zero_entries] = 0.0
+        K = K + sp.diags(self.cmask.astype(float))
+        rhs[self.cdofs] = duc
+        return spla.splu(K.tocsc()).solve(rhs)
+
+    def step(self):
+        """One increment: max_newton assemble+solve passes, then the commit."""
+        mesh = self.mesh
+        for it in range(self.max_newton):
+            Ke, Re, st = self.be.assemble(self.u[mesh.cell_dofs], self.F_e, self.F_r)
+            K = mesh.assemble_matrix(Ke)
+            R = mesh.assemble_vector(Re)
+            duc = self.cvals if it == 0 else np.zeros_like(self.cvals)
+            self.u += self._solve(K, R, duc)
+        F = mesh.deformation_gradients(self.u)
+        self.be.update(F, 0, self.F_e, self.F_r)
+        avg = self.be.averages()
+        self.be.reorient()
+        self.be.commit()
+        if self.multiphase:
+            self.F_e = self.F_r = 0.0
+        else:
+            self.F_r, self.F_e = float(avg[18]), float(avg[19])
+        E = avg[0:9].reshape(3, 3)
+        T = avg[9:18].reshape(3, 3)
+        row = [E[0, 0], E[1, 1], E[2, 2], E[1, 2], E[0, 2], E[0, 1],
+               T[0, 0], T[1, 1], T[2, 2], T[1, 2], T[0, 2], T[0, 1], avg[18], avg[19], avg[20]]
+        self.rows.append(row)
+        return row
+
+    def run(self, n_steps=None, callback=None):
+        n_steps = self.n_increments if n_steps is None else n_steps
+        for i in range(n_steps):
+            row = self.step()
+            if callback:
+                callback(i, row)
+        return np.array(self.rows)
+
+
+def kat_setup(fixture, backend_factory, material_from_fixture):
+    """Build mesh/backend/harness for a tests/golden/kat_*.npz fixture."""
+    d = dict(np.load(fixture))
+    mesh = StructuredMesh(tuple(int(x) for x in d["n_elem"]))
+    mat = material_from_fixture(d)
+    n_inc = int(round(float(d["total_T"]) / float(d["delT"])))
+    be = backend_factory([mat], d)
+    rod = np.repeat(d["cell_rodrigues"], 8, axis=0)
+    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+    h = NewtonHarness(be, mesh, d["bc"], n_inc, int(d["max_newton"]))
+    return h, d
