@@ -1,0 +1,418 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 crystal-plasticity qp hot path.
+
+Workload (one step): one batched calculatePlasticity with the algorithmic
+tangent (StiffnessCalFlag = 1, dP/dF written out) over 2^21 quadrature points
+shuffled 50 % FCC (12+1 systems), 30 % BCC (48+1), 20 % HCP (24 slip + 6
+twins), each with a seeded random orientation and a history built by 10 prior
+committed increments of random loading F <- F (I + 2e-4 G), G ~ N(0,1)^{3x3}
+iid per qp; the timed increment is the next such F.  Synthetic data.
+
+Metric: qp-updates/s (whole job).  ``value`` is timed on device-resident
+inputs (CUDA events on the library's stream); ``e2e`` is the same step through
+the public host-pointer call cp_update with page-locked host buffers (F in;
+P, dP/dF, status out).  Inputs, outputs and state (~3 GB) are far larger than
+the 126 MB L2, so no flush is needed between steps.
+
+``--impl reference`` times the reference algorithm on the host cores instead:
+the reference cannot be built here (deal.II/PETSc/p4est/MPI absent), so its
+CPU implementation is the FP64 restatement under oracle/ (OpenMP over qps) on
+a bounded sample of the same workload.
+
+Run:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+      torchrun --nproc-per-node N bench.py --gpus N ...   (N independent replicas)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_QP = 1 << 21
+MIX = (0.5, 0.3, 0.2)
+SEED_LATTICE, SEED_ORIENT, SEED_LOAD = 1, 0, 2
+PRIOR_STEPS = 10
+AMP = 2e-4
+METRIC = "qp-updates/s (calculatePlasticity + dP/dF, FP64)"
+
+
+# --------------------------------------------------------------------- workload
+def lattice_ids(n, rank=0):
+    rng = np.random.default_rng(SEED_LATTICE + 1000 * rank)
+    n_fcc = int(round(MIX[0] * n))
+    n_bcc = int(round(MIX[1] * n))
+    lid = np.concatenate([np.zeros(n_fcc), np.ones(n_bcc), np.full(n - n_fcc - n_bcc, 2)]).astype(np.int32)
+    rng.shuffle(lid)
+    return lid
+
+
+def orientations(n, rank=0):
+    from plasticity_b200 import materials as M
+    return M.random_rodrigues(np.random.default_rng(SEED_ORIENT + 1000 * rank), n)
+
+
+def materials():
+    from plasticity_b200 import materials as M
+    return [M.fcc_cu(), M.bcc_48(), M.hcp_mg()]
+
+
+def flops_per_qp(n, p, rounds, e, c, flag):
+    """FP64 flops of one qp-update: 2 [U + flag T] with
+    U = 892 + 171n + 11n^2 + (2/3 p^3 + p^2) rounds + 27e and
+    T = 4374 + 27c + p (420 + 18c^3 + 27e) + 18p^2 + p^3  (FMA-equivalents)."""
+    p = p.astype(np.float64)
+    U = 892 + 171 * n + 11 * n * n + (2.0 / 3.0 * p ** 3 + p ** 2) * np.maximum(rounds, 1) * (p > 0) + 27 * e
+    T = 4374 + 27 * c + p * (420 + 18 * c ** 3 + 27 * e) + 18 * p ** 2 + p ** 3
+    return 2.0 * (U + flag * T)
+
+
+def bytes_per_qp(n, ns, nw, flag):
+    """Minimal HBM bytes of one qp-update as the bench calls it: reads F, Fp,
+    s, W, rotation, twin/slip fractions, twin flag; writes Fp, Fe, s, W,
+    fractions, P, status and (flag 1) dP/dF."""
+    rd = 8 * (9 + 9 + 2 * n + 3 + nw + ns) + 4
+    wr = 8 * (9 + 9 + 2 * n + nw + ns + 9) + 4 + (648 if flag else 0)
+    return rd + wr
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- CPU legs
+def cpu_sample_inputs(n_sample, rank=0):
+    """A bounded sample of the workload for the host runs: the first n_sample
+    qps (same lattice mix, orientations), history from 10 prior increments
+    drawn with a host RNG."""
+    lid = lattice_ids(N_QP, rank)[:n_sample]
+    rod = orientations(N_QP, rank)[:n_sample]
+    return lid, rod
+
+
+def run_oracle_sample(lid, rod, steps_prior, rng, threads):
+    from oracle import oracle as O
+    from plasticity_b200.capi import default_options
+    be = O.OracleBackend(materials(), default_options(), nthreads=threads)
+    be.bind_qps(lid, rod)
+    F = np.tile(np.eye(3).ravel(), (len(lid), 1))
+    for _ in range(steps_prior):
+        F = (F.reshape(-1, 3, 3) @ (np.eye(3) + AMP * rng.standard_normal((len(lid), 3, 3)))).reshape(-1, 9)
+        be.update(F, 0)
+        be.commit()
+    Fn = (F.reshape(-1, 3, 3) @ (np.eye(3) + AMP * rng.standard_normal((len(lid), 3, 3)))).reshape(-1, 9)
+    return be, Fn
+
+
+def reference_arm(args):
+    """The reference algorithm on the host cores (the oracle port; the
+    reference itself cannot be built without deal.II/PETSc/p4est/MPI)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n_s = args.cpu_sample
+    lid, rod = cpu_sample_inputs(n_s)
+    be, Fn = run_oracle_sample(lid, rod, PRIOR_STEPS, np.random.default_rng(SEED_LOAD), threads)
+    for _ in range(args.warmup):
+        be.update(Fn, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        be.update(Fn, 1)
+    dt = time.perf_counter() - t0
+    v = n_s * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "qp-updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"mixed FCC/BCC/HCP qps 50/30/20, flag 1, sample {n_s} of {N_QP}",
+                   "n_qp": n_s, "stiffness_flag": 1, "prior_increments": PRIOR_STEPS},
+        "cpu_baseline": {"value": v, "unit": "qp-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"first {n_s} qps of the {N_QP}-qp workload, one flag-1 update per step"},
+        "e2e": {"value": v, "unit": "qp-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference (deal.II/PETSc/p4est/MPI) not buildable here; timed its FP64 CPU restatement (oracle/)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------- GPU arm
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    from plasticity_b200 import capi
+    from plasticity_b200.capi import CpHandle, default_options
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n = args.n_qp
+    lid = lattice_ids(n, rank)
+    rod = orientations(n, rank)
+    mats = materials()
+    h = CpHandle(mats, default_options(device=local))
+    h.bind_qps(lid, rod)
+    stream = torch.cuda.ExternalStream(h.stream(), device=dev)
+
+    # history: PRIOR_STEPS committed increments of random loading (untimed)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED_LOAD + 1000 * rank)
+    eye = torch.eye(3, dtype=torch.float64, device=dev)
+    F = eye.expand(n, 3, 3).contiguous()
+    P = torch.empty(n, 9, dtype=torch.float64, device=dev)
+    dPdF = torch.empty(n, 81, dtype=torch.float64, device=dev)
+    status = torch.empty(n, dtype=torch.int32, device=dev)
+    for _ in range(PRIOR_STEPS):
+        G = torch.randn(n, 3, 3, dtype=torch.float64, device=dev, generator=gen)
+        F = F @ (eye + AMP * G)
+        torch.cuda.synchronize()
+        h.update_device(F.data_ptr(), 0, 0.0, 0.0, P.data_ptr(), None, None, status.data_ptr())
+        h.commit()
+        h.synchronize()
+    G = torch.randn(n, 3, 3, dtype=torch.float64, device=dev, generator=gen)
+    Fn = (F @ (eye + AMP * G)).contiguous()
+    torch.cuda.synchronize()
+
+    def step():
+        h.update_device(Fn.data_ptr(), 1, 0.0, 0.0, P.data_ptr(), None, dPdF.data_ptr(), status.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    h.synchronize()
+    st = status.cpu().numpy()
+    bad = int(np.count_nonzero(st & capi.CP_QP_ERROR_MASK))
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    h.synchronize()
+    h.set_timing(True)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    elapsed_ms = e0.elapsed_time(e1)
+    timing = h.get_timing()
+    h.set_timing(False)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * n * args.steps / (elapsed_ms * 1e-3)
+
+    # roofline of the dominant kernel (the group with the largest time)
+    stats = h.stats()
+    dom = max(timing, key=lambda g: g[3])
+    dom_lat = dom[0]
+    lat_n = {i: (m.n_total, m.n_slip, m.n_twin) for i, m in enumerate(mats)}
+    sel = stats[:, 6] == dom_lat
+    nT, ns, nw = lat_n[dom_lat]
+    fl = flops_per_qp(nT, stats[sel, 1], stats[sel, 2], stats[sel, 3], stats[sel, 4], 1).sum()
+    by = bytes_per_qp(nT, ns, nw, 1) * int(sel.sum())
+    dom_ms = dom[3] / max(dom[2], 1)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    fp64_peak = capi.measure_fp64_peak(local)
+    lat_name = ["fcc", "bcc", "hcp"][dom_lat]
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if os.path.exists(tf):
+        for ln in open(tf):
+            f = ln.split()
+            if len(f) >= 2 and f[0] == f"update_{lat_name}":
+                traffic = float(f[1]) * int(sel.sum())
+    all_fl = sum(flops_per_qp(lat_n[L][0], stats[stats[:, 6] == L, 1], stats[stats[:, 6] == L, 2],
+                              stats[stats[:, 6] == L, 3], stats[stats[:, 6] == L, 4], 1).sum() for L in range(3))
+
+    # e2e through the public host-pointer call with page-locked buffers
+    e2e = None
+    if not args.no_e2e:
+        hF = torch.empty(n, 9, dtype=torch.float64, pin_memory=True)
+        hF.copy_(Fn.reshape(n, 9).cpu())
+        hP = torch.empty(n, 9, dtype=torch.float64, pin_memory=True)
+        hD = torch.empty(n, 81, dtype=torch.float64, pin_memory=True)
+        hS = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        import ctypes as C
+        dp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))
+        ip = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_int32))
+        call = lambda: h.lib.cp_update(h.h, dp(hF), 1, 0.0, 0.0, dp(hP), None, dp(hD), ip(hS))
+        for _ in range(max(1, args.warmup)):
+            assert call() == 0
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            assert call() == 0
+        dt = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([dt], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": world * n * args.steps / dt, "unit": "qp-updates/s",
+               "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": (9 + 81) * 8 * n + 4 * n,
+               "ms_per_step": 1e3 * dt / args.steps}
+
+    # CPU baseline and a live parity check on a bounded sample (rank 0, N=1)
+    cpu = None
+    parity = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, parity = cpu_leg(args, h, Fn, P, dPdF, lid, rod)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "qp-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "2^21 shuffled qps 50% FCC(12+1) / 30% BCC(48+1) / 20% HCP(24+6), "
+                               "history of 10 random increments F<-F(I+2e-4 G), one flag-1 update per step",
+                   "n_qp_per_gpu": n, "stiffness_flag": 1, "parallelism": f"replicas x{world}",
+                   "l2": "inputs+outputs+state ~3 GB >> 126 MB L2 (no flush needed)"},
+        "clocks": clk,
+        "e2e": e2e,
+        "gpu_launches": args.steps * len(timing),
+        "roofline": {"bound": "hbm", "kernel": f"update_kernel[{lat_name}]", "achieved": by / (dom_ms * 1e-3) / 1e9,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": by / (dom_ms * 1e-3) / 1e9 / hbm_peak,
+                     "traffic": traffic, "algorithmic_bytes": by, "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"},
+        "roofline_fp64": {"bound": "fp64", "kernel": f"update_kernel[{lat_name}]",
+                          "achieved": fl / (dom_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                          "frac": fl / (dom_ms * 1e-3) / 1e12 / fp64_peak,
+                          "peak_source": "measured FP64 FMA probe (cp_measure_fp64_peak), live",
+                          "all_kernels_achieved": all_fl / (ms_per_step * 1e-3) / 1e12},
+        "kernels": [{"lattice": ["fcc", "bcc", "hcp"][g[0]], "n_qp": g[1], "ms_per_launch": g[3] / max(g[2], 1)}
+                    for g in timing],
+        "qp_error_flags": bad,
+        "cpu_baseline": cpu,
+        "parity": parity,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
+    """Oracle on the first qps of this exact workload: the GPU's conv state of
+    those qps and the same F; times one flag-1 update on all host cores and
+    compares it with the GPU's P and dP/dF for those qps."""
+    from oracle import oracle as O
+    from plasticity_b200.capi import default_options
+    n_s = args.cpu_sample
+    threads = os.cpu_count() or 1
+    be = O.OracleBackend(materials(), default_options(), nthreads=threads)
+    be.bind_qps(lid[:n_s], rod[:n_s])
+    for f in ("Fp", "Fe", "s", "W", "rot", "rotnew", "twinfrac", "slipfrac", "twin"):
+        for suf in ("_conv", "_iter"):
+            be.set_state(f + suf, h.get_state(f + suf)[:n_s])
+    Fh = Fn.reshape(-1, 9)[:n_s].cpu().numpy()
+    t0 = time.perf_counter()
+    Po, _, Do, so = be.update(Fh, 1)
+    dt = time.perf_counter() - t0
+    Pg = P[:n_s].cpu().numpy()
+    Dg = dPdF[:n_s].cpu().numpy()
+    sg = h.stats()[:n_s]
+    so_ = be.stats()
+
+    def rel(a, b):
+        return float((np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)).max())
+
+    parity = {"sample_qps": n_s, "max_rel_err_P": rel(Pg, Po), "max_rel_err_dPdF": rel(Dg, Do),
+              "active_sets_identical": bool(np.array_equal(sg[:, :3], so_[:, :3])), "tolerance": 1e-10}
+    cpu = {"value": n_s / dt, "unit": "qp-updates/s", "cores": threads, "kind": "port",
+           "sample": f"first {n_s} qps of the workload (GPU's history, same F), one flag-1 update"}
+    return cpu, parity
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n-qp", type=int, default=N_QP)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 16)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

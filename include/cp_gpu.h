@@ -20,9 +20,9 @@
  *   - Every function returns an int status: CP_OK (0) or a negative CP_E* code;
  *     cp_last_error() gives a one-line message for the handle's last failure.
  *   - Pointers named h_* are host pointers, borrowed for the duration of the
- *     call (they may be pageable; the library stages them through its own
- *     pinned buffers).  Pointers named d_* are device pointers on the handle's
- *     GPU; those calls are asynchronous on the handle's stream unless noted.
+ *     call (pageable works; page-locked memory gets the full copy bandwidth).
+ *     Pointers named d_* are device pointers on the handle's GPU; those calls
+ *     are asynchronous on the handle's stream unless noted.
  *   - 3x3 tensors are row-major (A[i][j] at 3*i+j); a batch of tensors is
  *     qp-major: qp k's tensor starts at 9*k.  dP/dF is dPdF[m][n][o][p] at
  *     81*k + 27*m + 9*n + 3*o + p (the reference's Tensor<4,3> dP_dF).
@@ -221,6 +221,24 @@ int cp_set_state(cp_handle* h, int32_t field, const double* h_buf);
 
 /* Wait for all work queued on the handle's stream. */
 int cp_synchronize(cp_handle* h);
+
+/* Diagnostics: when enabled, every update/assembly kernel launch is
+ * bracketed by CUDA events on the handle's stream; cp_get_timing returns, per
+ * lattice group (internal qp groups, one per lattice present), its lattice
+ * id, qp count, number of timed launches and their summed duration in ms,
+ * and the number of groups.  cp_set_timing resets the accumulators. */
+int cp_set_timing(cp_handle* h, int32_t enable);
+int cp_get_timing(cp_handle* h, int32_t max_groups, int32_t* lattice, int64_t* count,
+                  int64_t* launches, double* total_ms);
+
+/* Diagnostics: measured FP64 FMA throughput of the device (TFLOP/s), the
+ * denominator of the FP64 roofline of the qp update (no counterpart in the
+ * reference). */
+int cp_measure_fp64_peak(int32_t device, double* tflops);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own
+ * device work (input uploads, output reads) with the *_device entry points. */
+void* cp_stream(cp_handle* h);
 
 #ifdef __cplusplus
 }

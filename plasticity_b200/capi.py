@@ -160,6 +160,9 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_set_state": (C.c_int, [H, C.c_int32, D]),
         "cp_synchronize": (C.c_int, [H]),
         "cp_stream": (C.c_void_p, [H]),
+        "cp_measure_fp64_peak": (C.c_int, [C.c_int32, D]),
+        "cp_set_timing": (C.c_int, [H, C.c_int32]),
+        "cp_get_timing": (C.c_int, [H, C.c_int32, I32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -168,6 +171,15 @@ def load_library(path: str | None = None) -> C.CDLL:
     if path is None:
         _lib = lib
     return lib
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    lib = load_library()
+    out = C.c_double()
+    rc = lib.cp_measure_fp64_peak(device, C.byref(out))
+    if rc != CP_OK:
+        raise CpError(f"cp_measure_fp64_peak failed ({rc})")
+    return float(out.value)
 
 
 class CpHandle:
@@ -287,3 +299,19 @@ class CpHandle:
 
     def stream(self) -> int:
         return int(self.lib.cp_stream(self.h) or 0)
+
+    def set_timing(self, enable: bool):
+        self._check(self.lib.cp_set_timing(self.h, 1 if enable else 0), "cp_set_timing")
+
+    def get_timing(self):
+        """[(lattice, qp count, launches, total ms)] per internal group."""
+        m = CP_MAX_LATTICES
+        lat = np.zeros(m, np.int32)
+        cnt = np.zeros(m, np.int64)
+        lau = np.zeros(m, np.int64)
+        ms = np.zeros(m)
+        ng = self.lib.cp_get_timing(self.h, m, iptr(lat), cnt.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    lau.ctypes.data_as(C.POINTER(C.c_int64)), dptr(ms))
+        if ng < 0:
+            self._check(ng, "cp_get_timing")
+        return [(int(lat[g]), int(cnt[g]), int(lau[g]), float(ms[g])) for g in range(ng)]

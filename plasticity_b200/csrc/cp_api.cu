@@ -1,0 +1,982 @@
+// cp_api.cu -- C ABI of include/cp_gpu.h: resident per-qp history on one
+// GPU, kernel dispatch by lattice class, host/device entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cp_gpu.h"
+#include "cp_kernels.cuh"
+
+using namespace cp;
+
+// ---------------------------------------------------------------- kernels
+namespace cp {
+
+__global__ void init_state_kernel(const LatDev* __restrict__ L, GroupDev g, const double* __restrict__ rod) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.count) return;
+    const int64_t cnt = g.count;
+    const int n = L->n, ns = L->ns, nw = L->nw;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        const double v = (c == 0 || c == 4 || c == 8) ? 1.0 : 0.0;
+        g.Fp_c[c * cnt + i] = v;
+        g.Fe_c[c * cnt + i] = v;
+        g.Fp_i[c * cnt + i] = v;
+        g.Fe_i[c * cnt + i] = v;
+    }
+    for (int a = 0; a < n; ++a) {
+        const double s0 = L->s0[a];
+        g.s_c[a * cnt + i] = s0;
+        g.s_i[a * cnt + i] = s0;
+        g.W_c[a * cnt + i] = 0.0;
+        g.W_i[a * cnt + i] = 0.0;
+    }
+    const int64_t k = g.qp[i];
+    for (int c = 0; c < 3; ++c) {
+        const double r = rod[3 * k + c];
+        g.rot_c[c * cnt + i] = r;
+        g.rot_i[c * cnt + i] = r;
+        g.rotnew_c[c * cnt + i] = r;
+        g.rotnew_i[c * cnt + i] = r;
+    }
+    for (int t = 0; t < nw; ++t) {
+        g.tw_c[t * cnt + i] = 0.0;
+        g.tw_i[t * cnt + i] = 0.0;
+    }
+    for (int t = 0; t < ns; ++t) {
+        g.sl_c[t * cnt + i] = 0.0;
+        g.sl_i[t * cnt + i] = 0.0;
+    }
+    g.twin_c[i] = 0;
+    g.twin_i[i] = 0;
+}
+
+// symmetric 3x3 eigen-decomposition by cyclic Jacobi (columns of V are
+// eigenvectors), the stand-in for LAPACK syevx of reorient.cc:35,48
+__device__ void eig_sym3(const M3& C, double ev[3], M3& V) {
+    M3 A = C;
+    V = eye3();
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        const double off = A(0, 1) * A(0, 1) + A(0, 2) * A(0, 2) + A(1, 2) * A(1, 2);
+        const double dia = A(0, 0) * A(0, 0) + A(1, 1) * A(1, 1) + A(2, 2) * A(2, 2);
+        if (off <= 1e-32 * dia || off == 0.0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                const double apq = A(p, q);
+                if (apq == 0.0) continue;
+                const double theta = (A(q, q) - A(p, p)) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    const double akp = A(k, p), akq = A(k, q);
+                    A(k, p) = c * akp - s * akq;
+                    A(k, q) = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double apk = A(p, k), aqk = A(q, k);
+                    A(p, k) = c * apk - s * aqk;
+                    A(q, k) = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double vkp = V(k, p), vkq = V(k, q);
+                    V(k, p) = c * vkp - s * vkq;
+                    V(k, q) = s * vkp + c * vkq;
+                }
+            }
+    }
+    ev[0] = A(0, 0);
+    ev[1] = A(1, 1);
+    ev[2] = A(2, 2);
+}
+
+__device__ M3 polar_rotation(const M3& Fe) {
+    const M3 C = mulTN(Fe, Fe);
+    double ev[3];
+    M3 V;
+    eig_sym3(C, ev, V);
+    M3 Lam = zero3();
+    Lam(0, 0) = sqrt(ev[0]);
+    Lam(1, 1) = sqrt(ev[1]);
+    Lam(2, 2) = sqrt(ev[2]);
+    const M3 U = mulNT(mul(V, Lam), V);
+    return mul(Fe, inv(U));
+}
+
+__global__ void reorient_kernel(GroupDev g) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.count) return;
+    const int64_t cnt = g.count;
+    double rold[3];
+    for (int c = 0; c < 3; ++c) rold[c] = g.rotnew_i[c * cnt + i];  // rotnew_conv = rotnew_iter
+    M3 Fe_old = load_soa3(g.Fe_c, cnt, i);
+    const M3 Fe_new = load_soa3(g.Fe_i, cnt, i);
+    if (g.twin_c[i] != g.twin_i[i]) Fe_old = Fe_new;
+    const M3 R_old = polar_rotation(Fe_old);
+    const M3 R_new = polar_rotation(Fe_new);
+    M3 Om = R_new;
+    axpy(Om, -1.0, R_old);
+    Om = mulNT(Om, R_new);
+    double ov[3];
+    ov[0] = -0.5 * (Om(1, 2) - Om(2, 1));
+    ov[1] = 0.5 * (Om(0, 2) - Om(2, 0));
+    ov[2] = -0.5 * (Om(0, 1) - Om(1, 0));
+    const double dot = ov[0] * rold[0] + ov[1] * rold[1] + ov[2] * rold[2];
+    double cr[3], rn[3];
+    cr[0] = ov[1] * rold[2] - ov[2] * rold[1];
+    cr[1] = ov[2] * rold[0] - ov[0] * rold[2];
+    cr[2] = ov[0] * rold[1] - ov[1] * rold[0];
+    for (int c = 0; c < 3; ++c) rn[c] = rold[c] + 0.5 * (ov[c] + dot * rold[c] + cr[c]);
+    const double mx = 10000.0;
+    const double nrm = sqrt(rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2]);
+    if (nrm > mx)
+        for (int c = 0; c < 3; ++c) rn[c] = rn[c] * mx / nrm;
+    for (int c = 0; c < 3; ++c) {
+        g.rotnew_c[c * cnt + i] = rn[c];
+        g.rotnew_i[c * cnt + i] = rn[c];  // rotnew_iter = rotnew_conv
+    }
+}
+
+constexpr int AVG_N = 22;
+constexpr int AVG_BLOCK = 256;
+
+__global__ void __launch_bounds__(AVG_BLOCK)
+    averages_partial_kernel(const LatDev* __restrict__ L, GroupDev g, const double* __restrict__ keepF,
+                            const double* __restrict__ keepT, const double* __restrict__ JxW, int uniform,
+                            double* __restrict__ partial) {
+    __shared__ double red[AVG_BLOCK / 32][AVG_N];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v[AVG_N];
+#pragma unroll
+    for (int c = 0; c < AVG_N; ++c) v[c] = 0.0;
+    if (i < g.count) {
+        const int64_t cnt = g.count;
+        const int64_t k = g.qp[i];
+        const double w = uniform ? JxW[k & 7] : JxW[k];
+        M3 F;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) F.a[c] = keepF[9 * k + c];
+        const M3 C = mulTN(F, F);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) v[3 * a + b] = 0.5 * (C(a, b) - (a == b ? 1.0 : 0.0)) * w;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) v[9 + c] = keepT[9 * k + c] * w;
+        double fr = 0.0, fs = 0.0;
+        for (int t = 0; t < L->nw; ++t) fr += g.tw_i[t * cnt + i];
+        for (int t = 0; t < L->ns; ++t) fs += g.sl_i[t * cnt + i];
+        v[18] = fr * w;
+        v[19] = (double)g.twin_i[i] * w;
+        v[20] = fs * w;
+        v[21] = w;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < AVG_N; ++c) {
+        double x = v[c];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) red[warp][c] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < AVG_N) {
+        double s = 0.0;
+        for (int wi = 0; wi < AVG_BLOCK / 32; ++wi) s += red[wi][threadIdx.x];
+        partial[(int64_t)blockIdx.x * AVG_N + threadIdx.x] = s;
+    }
+}
+
+__global__ void averages_final_kernel(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+    // one thread per component, fixed order: deterministic
+    const int c = threadIdx.x;
+    if (c >= AVG_N) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[(int64_t)b * AVG_N + c];
+    out[c] = s;
+}
+
+// gather one history field of a group into caller-order rows of width w
+__global__ void gather_field_kernel(const double* __restrict__ src, const int* __restrict__ isrc, int64_t cnt,
+                                    const int64_t* __restrict__ qp, int comps, int width,
+                                    double* __restrict__ dst) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    const int64_t k = qp[i];
+    for (int c = 0; c < width; ++c) {
+        double v = 0.0;
+        if (c < comps) v = isrc ? (double)isrc[c * cnt + i] : src[c * cnt + i];
+        dst[k * width + c] = v;
+    }
+}
+__global__ void scatter_field_kernel(double* __restrict__ dst, int* __restrict__ idst, int64_t cnt,
+                                     const int64_t* __restrict__ qp, int comps, int width,
+                                     const double* __restrict__ src) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cnt) return;
+    const int64_t k = qp[i];
+    for (int c = 0; c < comps; ++c) {
+        const double v = src[k * width + c];
+        if (idst)
+            idst[c * cnt + i] = (int)v;
+        else
+            dst[c * cnt + i] = v;
+    }
+}
+
+// FP64 FMA throughput probe: 8 independent dependent-FMA chains per thread.
+__global__ void fp64_fma_probe_kernel(int iters, double seed, double* out) {
+    double a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = seed + threadIdx.x * 1e-9 + c;
+    const double m = 0.999999999, k = 1e-12;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a[c] = fma(a[c], m, k);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s += a[c];
+    if (s == 12345.678) out[0] = s;  // keeps the chains alive
+}
+
+}  // namespace cp
+
+// ---------------------------------------------------------------- handle
+namespace {
+
+struct Group {
+    int lattice = 0;
+    int nt_class = 0;  // 16, 32 or 64
+    int n = 0, ns = 0, nw = 0;
+    int64_t count = 0;
+    int64_t* d_qp = nullptr;
+    double* d_block = nullptr;  // one allocation for all double fields
+    int* d_twin = nullptr;      // twin_c, twin_i
+    GroupDev dev{};
+};
+
+}  // namespace
+
+struct cp_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cp_options_t opts{};
+    Opts dopts{};
+    int n_lat = 0;
+    std::vector<cp_material_t> mats;
+    std::vector<LatDev*> d_lat;
+    int64_t n_qp = 0;
+    std::vector<int32_t> lattice_of;  // host copy, caller order
+    std::vector<Group> groups;
+    int n_max = 0, ns_max = 0, nw_max = 0;
+    // staging for host-pointer calls (caller order)
+    double *d_F = nullptr, *d_P = nullptr, *d_T = nullptr, *d_dPdF = nullptr;
+    int32_t* d_status = nullptr;
+    size_t dPdF_cap = 0;
+    int32_t* d_stats = nullptr;
+    double *d_keepF = nullptr, *d_keepT = nullptr;
+    bool have_post = false;
+    // mesh
+    int64_t n_cells = 0;
+    int uniform = 1;
+    double *d_gradN = nullptr, *d_JxW = nullptr;
+    double *d_U = nullptr, *d_Ke = nullptr, *d_Re = nullptr;
+    // averages scratch
+    double *d_avg_partial = nullptr, *d_avg_out = nullptr;
+    int64_t avg_cap = 0;
+    // optional per-launch timing of the update/assembly kernels
+    bool timing = false;
+    struct Pending {
+        cudaEvent_t a, b;
+        int group;
+    };
+    std::vector<Pending> pending;
+    std::vector<double> group_ms;
+    std::vector<int64_t> group_launches;
+    std::string err;
+};
+
+namespace {
+
+int fail(cp_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(cp_handle* h, cudaError_t e, const char* what) {
+    return fail(h, CP_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(h, call)                                            \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+int nt_class_of(int n) { return n <= 16 ? 16 : (n <= 32 ? 32 : 64); }
+
+void free_group(Group& g) {
+    cudaFree(g.d_qp);
+    cudaFree(g.d_block);
+    cudaFree(g.d_twin);
+    g = Group{};
+}
+
+void free_qps(cp_handle* h) {
+    for (auto& g : h->groups) free_group(g);
+    h->groups.clear();
+    cudaFree(h->d_F);
+    cudaFree(h->d_P);
+    cudaFree(h->d_T);
+    cudaFree(h->d_dPdF);
+    cudaFree(h->d_status);
+    cudaFree(h->d_stats);
+    cudaFree(h->d_keepF);
+    cudaFree(h->d_keepT);
+    h->d_F = h->d_P = h->d_T = h->d_dPdF = nullptr;
+    h->d_status = nullptr;
+    h->d_stats = nullptr;
+    h->d_keepF = h->d_keepT = nullptr;
+    h->dPdF_cap = 0;
+    h->n_qp = 0;
+    h->have_post = false;
+}
+
+void free_mesh(cp_handle* h) {
+    cudaFree(h->d_gradN);
+    cudaFree(h->d_JxW);
+    cudaFree(h->d_U);
+    cudaFree(h->d_Ke);
+    cudaFree(h->d_Re);
+    h->d_gradN = h->d_JxW = h->d_U = h->d_Ke = h->d_Re = nullptr;
+    h->n_cells = 0;
+}
+
+// double fields of a group in the order they are carved out of d_block
+int64_t group_doubles(int n, int ns, int nw, int64_t cnt) {
+    return cnt * 2 * (9 + 9 + n + n + 3 + 3 + nw + ns);
+}
+
+void carve(Group& g) {
+    const int64_t c = g.count;
+    double* p = g.d_block;
+    auto take = [&](int comps) {
+        double* r = p;
+        p += comps * c;
+        return r;
+    };
+    GroupDev& d = g.dev;
+    d.count = c;
+    d.qp = g.d_qp;
+    d.Fp_c = take(9);
+    d.Fe_c = take(9);
+    d.s_c = take(g.n);
+    d.W_c = take(g.n);
+    d.rot_c = take(3);
+    d.rotnew_c = take(3);
+    d.tw_c = take(g.nw);
+    d.sl_c = take(g.ns);
+    d.Fp_i = take(9);
+    d.Fe_i = take(9);
+    d.s_i = take(g.n);
+    d.W_i = take(g.n);
+    d.rot_i = take(3);
+    d.rotnew_i = take(3);
+    d.tw_i = take(g.nw);
+    d.sl_i = take(g.ns);
+    d.twin_c = g.d_twin;
+    d.twin_i = g.d_twin + c;
+}
+
+unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+template <int NT, int PMAX>
+void launch_update(cp_handle* h, const Group& g, const double* F, int flag, double F_e, double F_r, double* P,
+                   double* T, double* dPdF, int32_t* st, double* kF, double* kT) {
+    update_kernel<NT, PMAX><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(
+        h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P, T, dPdF, st, h->d_stats, kF, kT, g.lattice);
+}
+
+template <int NT, int PMAX>
+cudaError_t launch_assemble(cp_handle* h, const Group& g, const double* U, double F_e, double F_r, double* Ke,
+                            double* Re, int32_t* st) {
+    const size_t smem = (size_t)QP_BLOCK * 90 * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(assemble_kernel<NT, PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    assemble_kernel<NT, PMAX><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, smem, h->stream>>>(
+        h->d_lat[g.lattice], h->dopts, g.dev, U, h->d_gradN, h->d_JxW, h->uniform, F_e, F_r, Ke, Re, st,
+        h->d_stats, g.lattice);
+    return cudaGetLastError();
+}
+
+void timing_begin(cp_handle* h, int gi, cudaEvent_t* a) {
+    if (!h->timing) return;
+    cudaEventCreate(a);
+    cudaEventRecord(*a, h->stream);
+    (void)gi;
+}
+void timing_end(cp_handle* h, int gi, cudaEvent_t a) {
+    if (!h->timing) return;
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, h->stream);
+    h->pending.push_back({a, b, gi});
+}
+
+int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double F_r, double* P, double* T,
+                    double* dPdF, int32_t* st) {
+    double* kF = flag == 0 ? h->d_keepF : nullptr;
+    double* kT = flag == 0 ? h->d_keepT : nullptr;
+    for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+        const auto& g = h->groups[gi];
+        cudaEvent_t ev{};
+        timing_begin(h, (int)gi, &ev);
+        switch (g.nt_class) {
+            case 16: launch_update<16, 16>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
+            case 32: launch_update<32, 32>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
+            default: launch_update<64, 48>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
+        }
+        timing_end(h, (int)gi, ev);
+    }
+    CK(h, cudaGetLastError());
+    if (flag == 0) h->have_post = true;
+    return CP_OK;
+}
+
+int check_device(cp_handle* h) {
+    CK(h, cudaSetDevice(h->device));
+    return CP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+int cp_options_default(cp_options_t* o) {
+    if (!o) return CP_E_ARG;
+    std::memset(o, 0, sizeof *o);
+    o->stress_tolerance = 1.0e-9;
+    o->max_slip_search_iterations = 1;
+    o->max_solver_iterations = 1;
+    o->enable_multiphase = 0;
+    o->device = 0;
+    o->block_size = 0;
+    o->use_graphs = 1;
+    return CP_OK;
+}
+
+int cp_material_add_dummy_twin(cp_material_t* m) {
+    if (!m || m->n_slip < 1 || m->n_slip + 1 > CP_MAX_SYSTEMS) return CP_E_ARG;
+    const int d = m->n_slip;
+    m->n_twin = 1;
+    m->twinning_enabled = 0;
+    m->slip_normal[3 * d] = 1.0;
+    m->slip_normal[3 * d + 1] = 0.0;
+    m->slip_normal[3 * d + 2] = 0.0;
+    m->slip_direction[3 * d] = 0.0;
+    m->slip_direction[3 * d + 1] = 1.0;
+    m->slip_direction[3 * d + 2] = 0.0;
+    for (int j = 0; j < CP_MAX_SYSTEMS; ++j) {
+        m->latent_hardening[d * CP_MAX_SYSTEMS + j] = 0.0;
+        m->latent_hardening[j * CP_MAX_SYSTEMS + d] = 0.0;
+    }
+    m->initial_slip_resistance[d] = 10e14;
+    m->initial_hardening_modulus[d] = 1.0;
+    m->power_law_exponent[d] = 0.0;
+    m->saturation_stress[d] = 10e15;
+    m->kinematic_c1[d] = 0.0;
+    m->kinematic_c2[d] = 0.0;
+    return CP_OK;
+}
+
+int cp_create(const cp_material_t* lattices, int32_t n_lattices, const cp_options_t* opts, cp_handle** out) {
+    if (!out || !lattices || n_lattices < 1 || n_lattices > CP_MAX_LATTICES) return CP_E_ARG;
+    *out = nullptr;
+    for (int l = 0; l < n_lattices; ++l) {
+        const cp_material_t& m = lattices[l];
+        if (m.n_slip < 1 || m.n_twin < 1 || m.n_slip + m.n_twin > CP_MAX_SYSTEMS) return CP_E_ARG;
+    }
+    cp_handle* h = new cp_handle();
+    if (opts)
+        h->opts = *opts;
+    else
+        cp_options_default(&h->opts);
+    if (h->opts.max_slip_search_iterations < 0 || h->opts.max_solver_iterations < 0) {
+        delete h;
+        return CP_E_ARG;
+    }
+    h->device = h->opts.device;
+    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return CP_E_CUDA;
+    }
+    h->dopts.tol = h->opts.stress_tolerance;
+    h->dopts.max_search = h->opts.max_slip_search_iterations;
+    h->dopts.max_solver = h->opts.max_solver_iterations;
+    h->dopts.multiphase = h->opts.enable_multiphase;
+    h->n_lat = n_lattices;
+    h->mats.assign(lattices, lattices + n_lattices);
+    for (int l = 0; l < n_lattices; ++l) {
+        const cp_material_t& m = lattices[l];
+        LatDev hl;
+        std::memset(&hl, 0, sizeof hl);
+        hl.n = m.n_slip + m.n_twin;
+        hl.ns = m.n_slip;
+        hl.nw = m.n_twin;
+        hl.twinning = m.twinning_enabled;
+        std::memcpy(hl.C, m.elastic_stiffness, sizeof hl.C);
+        std::memcpy(hl.m, m.slip_direction, sizeof hl.m);
+        std::memcpy(hl.nn, m.slip_normal, sizeof hl.nn);
+        std::memcpy(hl.q, m.latent_hardening, sizeof hl.q);
+        std::memcpy(hl.s0, m.initial_slip_resistance, sizeof hl.s0);
+        std::memcpy(hl.h0, m.initial_hardening_modulus, sizeof hl.h0);
+        std::memcpy(hl.ss, m.saturation_stress, sizeof hl.ss);
+        std::memcpy(hl.a, m.power_law_exponent, sizeof hl.a);
+        std::memcpy(hl.C1, m.kinematic_c1, sizeof hl.C1);
+        std::memcpy(hl.C2, m.kinematic_c2, sizeof hl.C2);
+        hl.twin_thr = m.twin_threshold_fraction;
+        hl.twin_sat = m.twin_saturation_factor;
+        hl.twin_shear = m.twin_shear;
+        LatDev* d = nullptr;
+        if (cudaMalloc(&d, sizeof(LatDev)) != cudaSuccess ||
+            cudaMemcpy(d, &hl, sizeof hl, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(d);
+            cp_destroy(h);
+            return CP_E_CUDA;
+        }
+        h->d_lat.push_back(d);
+        h->n_max = std::max(h->n_max, hl.n);
+        h->ns_max = std::max(h->ns_max, hl.ns);
+        h->nw_max = std::max(h->nw_max, hl.nw);
+    }
+    *out = h;
+    return CP_OK;
+}
+
+void cp_destroy(cp_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_qps(h);
+    free_mesh(h);
+    cudaFree(h->d_avg_partial);
+    cudaFree(h->d_avg_out);
+    for (auto* d : h->d_lat) cudaFree(d);
+    for (auto& p : h->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char* cp_last_error(const cp_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+void* cp_stream(cp_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int64_t cp_num_qps(const cp_handle* h) { return h ? h->n_qp : 0; }
+
+int cp_bind_qps(cp_handle* h, int64_t n_qp, const int32_t* lattice_id, const double* rod) {
+    if (!h) return CP_E_ARG;
+    if (n_qp < 1 || !lattice_id || !rod) return fail(h, CP_E_ARG, "cp_bind_qps: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    std::vector<std::vector<int64_t>> idx(h->n_lat);
+    for (int64_t k = 0; k < n_qp; ++k) {
+        const int l = lattice_id[k];
+        if (l < 0 || l >= h->n_lat) return fail(h, CP_E_ARG, "cp_bind_qps: lattice id out of range");
+        idx[l].push_back(k);
+    }
+    free_qps(h);
+    free_mesh(h);
+    h->n_qp = n_qp;
+    h->lattice_of.assign(lattice_id, lattice_id + n_qp);
+    double* d_rod = nullptr;
+    CK(h, cudaMalloc(&d_rod, sizeof(double) * 3 * n_qp));
+    CK(h, cudaMemcpy(d_rod, rod, sizeof(double) * 3 * n_qp, cudaMemcpyHostToDevice));
+    for (int l = 0; l < h->n_lat; ++l) {
+        if (idx[l].empty()) continue;
+        Group g;
+        g.lattice = l;
+        g.ns = h->mats[l].n_slip;
+        g.nw = h->mats[l].n_twin;
+        g.n = g.ns + g.nw;
+        g.nt_class = nt_class_of(g.n);
+        g.count = (int64_t)idx[l].size();
+        if (cudaMalloc(&g.d_qp, sizeof(int64_t) * g.count) != cudaSuccess ||
+            cudaMalloc(&g.d_block, sizeof(double) * group_doubles(g.n, g.ns, g.nw, g.count)) != cudaSuccess ||
+            cudaMalloc(&g.d_twin, sizeof(int) * 2 * g.count) != cudaSuccess) {
+            free_group(g);
+            cudaFree(d_rod);
+            free_qps(h);
+            return fail(h, CP_E_NOMEM, "cp_bind_qps: device allocation failed");
+        }
+        CK(h, cudaMemcpy(g.d_qp, idx[l].data(), sizeof(int64_t) * g.count, cudaMemcpyHostToDevice));
+        carve(g);
+        init_state_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(h->d_lat[l], g.dev, d_rod);
+        h->groups.push_back(g);
+    }
+    CK(h, cudaGetLastError());
+    CK(h, cudaStreamSynchronize(h->stream));
+    cudaFree(d_rod);
+    if (cudaMalloc(&h->d_stats, sizeof(int32_t) * 8 * n_qp) != cudaSuccess ||
+        cudaMalloc(&h->d_keepF, sizeof(double) * 9 * n_qp) != cudaSuccess ||
+        cudaMalloc(&h->d_keepT, sizeof(double) * 9 * n_qp) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_bind_qps: device allocation failed");
+    CK(h, cudaMemset(h->d_stats, 0, sizeof(int32_t) * 8 * n_qp));
+    return CP_OK;
+}
+
+static int ensure_staging(cp_handle* h, bool need_dPdF) {
+    const int64_t n = h->n_qp;
+    if (!h->d_F) {
+        if (cudaMalloc(&h->d_F, sizeof(double) * 9 * n) != cudaSuccess ||
+            cudaMalloc(&h->d_P, sizeof(double) * 9 * n) != cudaSuccess ||
+            cudaMalloc(&h->d_T, sizeof(double) * 9 * n) != cudaSuccess ||
+            cudaMalloc(&h->d_status, sizeof(int32_t) * n) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "staging allocation failed");
+    }
+    if (need_dPdF && h->dPdF_cap < (size_t)n) {
+        cudaFree(h->d_dPdF);
+        h->d_dPdF = nullptr;
+        if (cudaMalloc(&h->d_dPdF, sizeof(double) * 81 * n) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "staging allocation failed");
+        h->dPdF_cap = (size_t)n;
+    }
+    return CP_OK;
+}
+
+int cp_update_device(cp_handle* h, const double* d_F, int32_t flag, double F_e, double F_r, double* d_P,
+                     double* d_T, double* d_dPdF, int32_t* d_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_update: no qps bound");
+    if (!d_F || (flag != 0 && flag != 1)) return fail(h, CP_E_ARG, "cp_update: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    return dispatch_update(h, d_F, flag, F_e, F_r, d_P, d_T, d_dPdF, d_status);
+}
+
+int cp_update(cp_handle* h, const double* h_F, int32_t flag, double F_e, double F_r, double* h_P, double* h_T,
+              double* h_dPdF, int32_t* h_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_update: no qps bound");
+    if (!h_F || (flag != 0 && flag != 1)) return fail(h, CP_E_ARG, "cp_update: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, flag == 1 && h_dPdF)) return rc;
+    const int64_t n = h->n_qp;
+    CK(h, cudaMemcpyAsync(h->d_F, h_F, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->stream));
+    double* dd = (flag == 1 && h_dPdF) ? h->d_dPdF : nullptr;
+    if (int rc = dispatch_update(h, h->d_F, flag, F_e, F_r, h_P ? h->d_P : nullptr, h_T ? h->d_T : nullptr, dd,
+                                 h->d_status))
+        return rc;
+    if (h_P) CK(h, cudaMemcpyAsync(h_P, h->d_P, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+    if (h_T) CK(h, cudaMemcpyAsync(h_T, h->d_T, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+    if (dd) CK(h, cudaMemcpyAsync(h_dPdF, dd, sizeof(double) * 81 * n, cudaMemcpyDeviceToHost, h->stream));
+    if (h_status)
+        CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+int cp_get_stats(cp_handle* h, int32_t* h_stats) {
+    if (!h || !h_stats) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "no qps bound");
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaMemcpyAsync(h_stats, h->d_stats, sizeof(int32_t) * 8 * h->n_qp, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+int cp_bind_mesh(cp_handle* h, int64_t n_cells, const double* grad_N, const double* JxW, int32_t uniform) {
+    if (!h) return CP_E_ARG;
+    if (n_cells < 1 || !grad_N || !JxW) return fail(h, CP_E_ARG, "cp_bind_mesh: bad arguments");
+    if (h->n_qp != 8 * n_cells) return fail(h, CP_E_STATE, "cp_bind_mesh: bound qps must be 8 per cell");
+    for (int64_t c = 0; c < n_cells; ++c)
+        for (int q = 1; q < 8; ++q)
+            if (h->lattice_of[8 * c + q] != h->lattice_of[8 * c])
+                return fail(h, CP_E_ARG, "cp_bind_mesh: the 8 qps of a cell must share a lattice");
+    if (int rc = check_device(h)) return rc;
+    free_mesh(h);
+    const size_t ng = uniform ? 192 : (size_t)192 * n_cells, nw = uniform ? 8 : (size_t)8 * n_cells;
+    if (cudaMalloc(&h->d_gradN, sizeof(double) * ng) != cudaSuccess ||
+        cudaMalloc(&h->d_JxW, sizeof(double) * nw) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_bind_mesh: allocation failed");
+    CK(h, cudaMemcpy(h->d_gradN, grad_N, sizeof(double) * ng, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->d_JxW, JxW, sizeof(double) * nw, cudaMemcpyHostToDevice));
+    h->n_cells = n_cells;
+    h->uniform = uniform ? 1 : 0;
+    return CP_OK;
+}
+
+int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, double* d_Ke, double* d_Re,
+                       int32_t* d_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble: no mesh bound");
+    if (!d_U || !d_Ke || !d_Re) return fail(h, CP_E_ARG, "cp_assemble: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+        const auto& g = h->groups[gi];
+        cudaEvent_t ev{};
+        timing_begin(h, (int)gi, &ev);
+        cudaError_t e;
+        switch (g.nt_class) {
+            case 16: e = launch_assemble<16, 16>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
+            case 32: e = launch_assemble<32, 32>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
+            default: e = launch_assemble<64, 48>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
+        }
+        timing_end(h, (int)gi, ev);
+        if (e != cudaSuccess) return cuda_fail(h, e, "assemble_kernel");
+    }
+    return CP_OK;
+}
+
+int cp_assemble(cp_handle* h, const double* h_U, double F_e, double F_r, double* h_Ke, double* h_Re,
+                int32_t* h_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble: no mesh bound");
+    if (!h_U || !h_Ke || !h_Re) return fail(h, CP_E_ARG, "cp_assemble: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    const int64_t nc = h->n_cells;
+    if (!h->d_U) {
+        if (cudaMalloc(&h->d_U, sizeof(double) * 24 * nc) != cudaSuccess ||
+            cudaMalloc(&h->d_Ke, sizeof(double) * 576 * nc) != cudaSuccess ||
+            cudaMalloc(&h->d_Re, sizeof(double) * 24 * nc) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "cp_assemble: allocation failed");
+    }
+    CK(h, cudaMemcpyAsync(h->d_U, h_U, sizeof(double) * 24 * nc, cudaMemcpyHostToDevice, h->stream));
+    if (int rc = cp_assemble_device(h, h->d_U, F_e, F_r, h->d_Ke, h->d_Re, h->d_status)) return rc;
+    CK(h, cudaMemcpyAsync(h_Ke, h->d_Ke, sizeof(double) * 576 * nc, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(h_Re, h->d_Re, sizeof(double) * 24 * nc, cudaMemcpyDeviceToHost, h->stream));
+    if (h_status)
+        CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * h->n_qp, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+int cp_averages(cp_handle* h, double out[22]) {
+    if (!h || !out) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_averages: no mesh bound (JxW needed)");
+    if (!h->have_post) return fail(h, CP_E_STATE, "cp_averages: no cp_update with stiffness_flag 0 yet");
+    if (int rc = check_device(h)) return rc;
+    int64_t nblocks = 0;
+    for (const auto& g : h->groups) nblocks += blocks_for(g.count, AVG_BLOCK);
+    if (h->avg_cap < nblocks) {
+        cudaFree(h->d_avg_partial);
+        h->d_avg_partial = nullptr;
+        if (cudaMalloc(&h->d_avg_partial, sizeof(double) * AVG_N * nblocks) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "cp_averages: allocation failed");
+        h->avg_cap = nblocks;
+    }
+    if (!h->d_avg_out && cudaMalloc(&h->d_avg_out, sizeof(double) * AVG_N) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_averages: allocation failed");
+    int64_t off = 0;
+    for (const auto& g : h->groups) {
+        const unsigned nb = blocks_for(g.count, AVG_BLOCK);
+        averages_partial_kernel<<<nb, AVG_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], g.dev, h->d_keepF, h->d_keepT,
+                                                                 h->d_JxW, h->uniform,
+                                                                 h->d_avg_partial + off * AVG_N);
+        off += nb;
+    }
+    averages_final_kernel<<<1, 32, 0, h->stream>>>(h->d_avg_partial, (int)nblocks, h->d_avg_out);
+    CK(h, cudaGetLastError());
+    double sums[AVG_N];
+    CK(h, cudaMemcpyAsync(sums, h->d_avg_out, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const double vol = sums[21];
+    for (int c = 0; c < 21; ++c) out[c] = sums[c] / vol;
+    out[21] = vol;
+    return CP_OK;
+}
+
+int cp_reorient(cp_handle* h) {
+    if (!h) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_reorient: no qps bound");
+    if (int rc = check_device(h)) return rc;
+    for (const auto& g : h->groups) reorient_kernel<<<blocks_for(g.count, 128), 128, 0, h->stream>>>(g.dev);
+    CK(h, cudaGetLastError());
+    return CP_OK;
+}
+
+int cp_commit(cp_handle* h) {
+    if (!h) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_commit: no qps bound");
+    if (int rc = check_device(h)) return rc;
+    for (const auto& g : h->groups) {
+        // the _iter half of the block directly follows the _conv half
+        const int64_t half = group_doubles(g.n, g.ns, g.nw, g.count) / 2;
+        CK(h, cudaMemcpyAsync(g.d_block, g.d_block + half, sizeof(double) * half, cudaMemcpyDeviceToDevice,
+                              h->stream));
+        CK(h, cudaMemcpyAsync(g.d_twin, g.d_twin + g.count, sizeof(int) * g.count, cudaMemcpyDeviceToDevice,
+                              h->stream));
+    }
+    return CP_OK;
+}
+
+static bool field_info(const cp_handle* h, const Group& g, int field, double** p, int** ip, int* comps) {
+    const bool it = field >= CP_FIELD_ITER_OFFSET;
+    const int f = it ? field - CP_FIELD_ITER_OFFSET : field;
+    const GroupDev& d = g.dev;
+    *ip = nullptr;
+    *p = nullptr;
+    switch (f) {
+        case CP_FIELD_FP_CONV: *p = it ? d.Fp_i : d.Fp_c; *comps = 9; break;
+        case CP_FIELD_FE_CONV: *p = it ? d.Fe_i : d.Fe_c; *comps = 9; break;
+        case CP_FIELD_S_CONV: *p = it ? d.s_i : d.s_c; *comps = g.n; break;
+        case CP_FIELD_W_CONV: *p = it ? d.W_i : d.W_c; *comps = g.n; break;
+        case CP_FIELD_ROT_CONV: *p = it ? d.rot_i : d.rot_c; *comps = 3; break;
+        case CP_FIELD_ROTNEW_CONV: *p = it ? d.rotnew_i : d.rotnew_c; *comps = 3; break;
+        case CP_FIELD_TWINFRAC_CONV: *p = it ? d.tw_i : d.tw_c; *comps = g.nw; break;
+        case CP_FIELD_SLIPFRAC_CONV: *p = it ? d.sl_i : d.sl_c; *comps = g.ns; break;
+        case CP_FIELD_TWIN_CONV: *ip = it ? d.twin_i : d.twin_c; *comps = 1; break;
+        default: return false;
+    }
+    (void)h;
+    return true;
+}
+
+int32_t cp_field_width(const cp_handle* h, int32_t field) {
+    if (!h) return 0;
+    const int f = field >= CP_FIELD_ITER_OFFSET ? field - CP_FIELD_ITER_OFFSET : field;
+    switch (f) {
+        case CP_FIELD_FP_CONV:
+        case CP_FIELD_FE_CONV: return 9;
+        case CP_FIELD_S_CONV:
+        case CP_FIELD_W_CONV: return h->n_max;
+        case CP_FIELD_ROT_CONV:
+        case CP_FIELD_ROTNEW_CONV: return 3;
+        case CP_FIELD_TWINFRAC_CONV: return h->nw_max;
+        case CP_FIELD_SLIPFRAC_CONV: return h->ns_max;
+        case CP_FIELD_TWIN_CONV: return 1;
+        default: return 0;
+    }
+}
+
+static int state_io(cp_handle* h, int32_t field, double* hbuf, bool get) {
+    if (!h || !hbuf) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "no qps bound");
+    const int width = cp_field_width(h, field);
+    if (width <= 0) return fail(h, CP_E_ARG, "unknown state field");
+    if (int rc = check_device(h)) return rc;
+    double* d_buf = nullptr;
+    CK(h, cudaMalloc(&d_buf, sizeof(double) * width * h->n_qp));
+    int rc = CP_OK;
+    if (get) {
+        CK(h, cudaMemsetAsync(d_buf, 0, sizeof(double) * width * h->n_qp, h->stream));
+    } else {
+        CK(h, cudaMemcpyAsync(d_buf, hbuf, sizeof(double) * width * h->n_qp, cudaMemcpyHostToDevice, h->stream));
+    }
+    for (const auto& g : h->groups) {
+        double* p;
+        int* ip;
+        int comps;
+        field_info(h, g, field, &p, &ip, &comps);
+        if (get)
+            gather_field_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(p, ip, g.count, g.d_qp, comps,
+                                                                               width, d_buf);
+        else
+            scatter_field_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(p, ip, g.count, g.d_qp, comps,
+                                                                                width, d_buf);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_fail(h, e, "state kernel");
+    if (get && rc == CP_OK)
+        e = cudaMemcpyAsync(hbuf, d_buf, sizeof(double) * width * h->n_qp, cudaMemcpyDeviceToHost, h->stream);
+    if (e != cudaSuccess && rc == CP_OK) rc = cuda_fail(h, e, "state copy");
+    cudaStreamSynchronize(h->stream);
+    cudaFree(d_buf);
+    return rc;
+}
+
+int cp_get_state(cp_handle* h, int32_t field, double* h_buf) { return state_io(h, field, h_buf, true); }
+int cp_set_state(cp_handle* h, int32_t field, const double* h_buf) {
+    return state_io(h, field, const_cast<double*>(h_buf), false);
+}
+
+int cp_measure_fp64_peak(int32_t device, double* tflops) {
+    if (!tflops) return CP_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return CP_E_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return CP_E_NOMEM;
+    const int threads = 256, blocks = sms * 8, iters = 1 << 15;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    fp64_fma_probe_kernel<<<blocks, threads>>>(256, 1.0, d);  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(e0);
+        fp64_fma_probe_kernel<<<blocks, threads>>>(iters, 1.0 + rep, d);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+    }
+    const cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) return CP_E_CUDA;
+    const double flops = 2.0 * 8.0 * (double)iters * threads * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return CP_OK;
+}
+
+int cp_set_timing(cp_handle* h, int32_t enable) {
+    if (!h) return CP_E_ARG;
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (auto& p : h->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    h->pending.clear();
+    h->timing = enable != 0;
+    h->group_ms.assign(h->groups.size(), 0.0);
+    h->group_launches.assign(h->groups.size(), 0);
+    return CP_OK;
+}
+
+int cp_get_timing(cp_handle* h, int32_t max_groups, int32_t* lattice, int64_t* count, int64_t* launches,
+                  double* total_ms) {
+    if (!h) return CP_E_ARG;
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (h->group_ms.size() != h->groups.size()) {
+        h->group_ms.assign(h->groups.size(), 0.0);
+        h->group_launches.assign(h->groups.size(), 0);
+    }
+    for (auto& p : h->pending) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        h->group_ms[p.group] += ms;
+        h->group_launches[p.group] += 1;
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    h->pending.clear();
+    const int ng = (int)h->groups.size();
+    for (int g = 0; g < ng && g < max_groups; ++g) {
+        if (lattice) lattice[g] = h->groups[g].lattice;
+        if (count) count[g] = h->groups[g].count;
+        if (launches) launches[g] = h->group_launches[g];
+        if (total_ms) total_ms[g] = h->group_ms[g];
+    }
+    return ng;
+}
+
+int cp_synchronize(cp_handle* h) {
+    if (!h) return CP_E_ARG;
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+}  // extern "C"

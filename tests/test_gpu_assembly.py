@@ -1,0 +1,83 @@
+"""Fused element assembly (getElementalValues) and the Newton drop-in on the
+GPU against the oracle, plus the reference's golden curve through the GPU."""
+import numpy as np
+import pytest
+
+from plasticity_b200 import harness as H
+from plasticity_b200 import materials as M
+from plasticity_b200.capi import CpHandle, default_options
+from tests._parity import TOL, copy_state, evolve, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _mesh_pair(oracle_lib, mats, cell_lattice, seed, steps):
+    mesh = H.StructuredMesh((4, 4, 4))
+    rng = np.random.default_rng(seed)
+    lid = np.repeat(np.asarray(cell_lattice, np.int32), 8)
+    rod = np.repeat(M.random_rodrigues(rng, mesh.n_cells), 8, axis=0)
+    ob = oracle_lib.OracleBackend(mats)
+    ob.bind_qps(lid, rod)
+    F = evolve(ob, np.tile(np.eye(3).ravel(), (len(lid), 1)), rng, steps)
+    gh = CpHandle(mats)
+    gh.bind_qps(lid, rod)
+    copy_state(ob, gh)
+    for be in (gh, ob):
+        be.bind_mesh(mesh.n_cells, mesh.grad_N, mesh.JxW, True)
+    return mesh, gh, ob, rng
+
+
+@pytest.mark.parametrize("mix", ["fcc", "bcc_hcp"])
+def test_assemble_parity(oracle_lib, cuda_lib, mix):
+    if mix == "fcc":
+        mats, cl = [M.fcc_cu()], np.zeros(64, np.int32)
+    else:
+        mats = [M.bcc_48(), M.hcp_mg()]
+        cl = (np.arange(64) % 3 == 0).astype(np.int32)
+    mesh, gh, ob, rng = _mesh_pair(oracle_lib, mats, cl, seed=3, steps=6)
+    # a displacement field: affine stretch + noise, large enough to yield
+    x = mesh.node_xyz
+    L = 2e-3 * rng.standard_normal((3, 3))
+    u = (x @ L.T).ravel() + 2e-4 * rng.standard_normal(mesh.n_dofs)
+    U = u[mesh.cell_dofs]
+    Kg, Rg, sg = gh.assemble(U)
+    Ko, Ro, so = ob.assemble(U)
+    assert np.array_equal(gh.stats()[:, 1], ob.stats()[:, 1])
+    assert (gh.stats()[:, 1] > 0).any()
+    assert rel_err(Kg, Ko) < TOL
+    assert rel_err(Rg, Ro) < TOL
+    for f in ("Fp_iter", "s_iter"):
+        assert rel_err(gh.get_state(f), ob.get_state(f)) < TOL
+    gh.close()
+
+
+def test_newton_dropin_matches_oracle_and_golden(oracle_lib, cuda_lib):
+    """The reference's fcc/simpleTension deck through the GPU drop-in: every
+    stress-strain row equals the oracle harness's and the golden curve."""
+    n_inc = 12
+
+    def gpu_factory(mats, d):
+        return CpHandle(mats, default_options(stress_tolerance=float(d["tol"])))
+
+    def cpu_factory(mats, d):
+        return oracle_lib.OracleBackend(mats, default_options(stress_tolerance=float(d["tol"])))
+
+    hg, d = H.kat_setup("tests/golden/kat_fcc_simpleTension.npz", gpu_factory, M.material_from_deck)
+    ho, _ = H.kat_setup("tests/golden/kat_fcc_simpleTension.npz", cpu_factory, M.material_from_deck)
+    rg = hg.run(n_inc)
+    ro = ho.run(n_inc)
+    assert rel_err(rg[:, :12], ro[:, :12]) < 1e-8
+    err = H.golden_errors(rg, d["golden"], n_inc)
+    assert err["stress"] < 1e-4 and err["strain"] < 1e-4 and err["slip"] < 1e-2, err
+    hg.be.close()
+
+
+def test_averages_match_oracle(oracle_lib, cuda_lib):
+    mesh, gh, ob, rng = _mesh_pair(oracle_lib, [M.hcp_mg()], np.zeros(64, np.int32), seed=9, steps=5)
+    F = np.tile(np.eye(3).ravel(), (mesh.n_cells * 8, 1))
+    F = (F.reshape(-1, 3, 3) @ (np.eye(3) + 1e-3 * rng.standard_normal((len(F), 3, 3)))).reshape(-1, 9)
+    gh.update(F, 0)
+    ob.update(F, 0)
+    a, b = gh.averages(), ob.averages()
+    assert np.allclose(a, b, rtol=1e-10, atol=1e-13 * np.abs(b).max())
+    gh.close()
