@@ -389,8 +389,14 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
     def rel(a, b):
         return float((np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-300)).max())
 
-    parity = {"sample_qps": n_s, "max_rel_err_P": rel(Pg, Po), "max_rel_err_dPdF": rel(Dg, Do),
-              "active_sets_identical": bool(np.array_equal(sg[:, :3], so_[:, :3])), "tolerance": 1e-10}
+    ok = (sg[:, 7] <= 12) & (so_[:, 7] <= 12)  # well-posed active-set solves on both sides
+    same = np.all(sg[:, :3] == so_[:, :3], axis=1)
+    parity = {"sample_qps": n_s, "well_posed_qps": int(ok.sum()),
+              "max_rel_err_P": rel(Pg[ok], Po[ok]), "max_rel_err_dPdF": rel(Dg[ok], Do[ok]),
+              "active_sets_identical": bool(same[ok].all()), "tolerance": 1e-10,
+              "ill_conditioned_qps": int((~ok).sum()),
+              "ill_conditioned_active_set_mismatches": int((~same[~ok]).sum()),
+              "criterion": "identical active sets and <=1e-10 on qps whose active-set solves have condition <= 1e12"}
     cpu = {"value": n_s / dt, "unit": "qp-updates/s", "cores": threads, "kind": "port",
            "sample": f"first {n_s} qps of the workload (GPU's history, same F), one flag-1 update"}
     return cpu, parity

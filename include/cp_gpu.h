@@ -60,6 +60,8 @@ extern "C" {
 #define CP_QP_ACTIVE_OVERFLOW 4 /* potentially active set larger than the kernel's tile */
 #define CP_QP_SERIES_CAP 8      /* exp / Gateaux series hit its term cap */
 #define CP_QP_SLIP_SEARCH_CAP 16 /* informational: slip-search cap reached (reference truncates silently, calculatePlasticity.cc:155-158) */
+#define CP_QP_ILL_CONDITIONED 32 /* informational: an active-set solve had condition > 1e12; the
+                                    reference's compute_inverse_svd(0.0) result there is set by rounding */
 
 /*
  * One lattice (phase).  Field names follow userInputParameters
@@ -157,7 +159,8 @@ int cp_update_device(cp_handle* h, const double* d_F, int32_t stiffness_flag,
  *   [0] potentially active systems p0, [1] final active systems p,
  *   [2] active-set removal rounds, [3] exp series terms e,
  *   [4] Gateaux series terms c (count3), [5] slip-search passes,
- *   [6] lattice id, [7] reserved.
+ *   [6] lattice id, [7] ceil(log10) of the largest condition estimate of the
+ *   active-set solves (pivot ratio of the LU factors; 0 when no solve ran).
  */
 int cp_get_stats(cp_handle* h, int32_t* h_stats);
 

@@ -315,7 +315,8 @@ int invert_n(const double* A, int n, double* B) {
  * LAPACKFullMatrix::compute_inverse_svd(0.0) (inactiveSlipRemoval.cc:26,99):
  * A = U S V^T, A^+ = V S^+ U^T, where singular values not above
  * threshold*max are treated as zero (threshold 0: only exact zeros). */
-int pinv_svd(const double* A, int n, double* Ainv) {
+int pinv_svd(const double* A, int n, double* Ainv, double* cond = nullptr) {
+    if (cond) *cond = 1.0;
     if (n == 0) return 0;
     std::vector<double> U(A, A + (size_t)n * n), V((size_t)n * n, 0.0), s(n);
     for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
@@ -356,6 +357,11 @@ int pinv_svd(const double* A, int n, double* Ainv) {
         smax = std::max(smax, s[i]);
     }
     const double threshold = 0.0;
+    if (cond) {
+        double smin = smax;
+        for (int i = 0; i < n; ++i) smin = std::min(smin, s[i]);
+        *cond = smin > 0.0 ? smax / smin : INFINITY;
+    }
     int sing = 0;
     std::vector<double> sinv(n);
     for (int i = 0; i < n; ++i) {
@@ -453,7 +459,8 @@ Lattice make_lattice(const cp_material_t* mat) {
  * by value in the reference; PA/n_PA are updated in place; x_old += x. */
 int inactive_slip_removal(int n, std::vector<int>& PA, const double* b,
                           const std::vector<double>& A, double* x_old, double* x,
-                          int* rounds) {
+                          int* rounds, double* maxcond) {
+    double cnd = 1.0;
     int sing = 0;
     int nPA = (int)PA.size();
     std::vector<double> Apa((size_t)nPA * nPA), Ainv((size_t)nPA * nPA), bpa(nPA), x1(n, 0.0);
@@ -461,7 +468,8 @@ int inactive_slip_removal(int n, std::vector<int>& PA, const double* b,
         bpa[i] = b[PA[i]];
         for (int j = 0; j < nPA; ++j) Apa[(size_t)i * nPA + j] = A[(size_t)PA[i] * NM + PA[j]];
     }
-    sing |= pinv_svd(Apa.data(), nPA, Ainv.data());
+    sing |= pinv_svd(Apa.data(), nPA, Ainv.data(), &cnd);
+    *maxcond = std::max(*maxcond, cnd);
     *rounds = 1;
     for (int i = 0; i < nPA; ++i) {
         double s = 0.0;
@@ -489,7 +497,8 @@ int inactive_slip_removal(int n, std::vector<int>& PA, const double* b,
             bpa[i] = b[PA[i]];
             for (int j = 0; j < m; ++j) Apa[(size_t)i * m + j] = A[(size_t)PA[i] * NM + PA[j]];
         }
-        sing |= pinv_svd(Apa.data(), m, Ainv.data());
+        sing |= pinv_svd(Apa.data(), m, Ainv.data(), &cnd);
+        *maxcond = std::max(*maxcond, cnd);
         ++*rounds;
         std::fill(x1.begin(), x1.end(), 0.0);
         nPA = m;
@@ -554,6 +563,7 @@ struct QpIO {
     const double* F;
     double *P, *T, *dPdF;
     int32_t* stats;
+    int32_t* status;
 };
 
 /* calculatePlasticity, calculatePlasticity.cc:13-1022, for qp k. */
@@ -624,6 +634,7 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
     M3 Ce_tau = zero3(), del_FP = zero3(), T_tau = zero3(), P_tau = zero3();
     double det_FE_tau, det_F_tau;
     int nPA = 0, p0 = -1, rounds_total = 0, e_terms = 0, c_terms = 0;
+    double maxcond = 1.0;
     unsigned iter1 = 1;
 
     while (iter1) {
@@ -714,7 +725,7 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
             if (count1 > (unsigned)opt.max_solver_iterations) break;
             for (int i = 0; i < n; ++i) x_beta[i] = 0.0;
             int rounds = 0;
-            if (inactive_slip_removal(n, PA, b, A, x_beta_old, x_beta, &rounds)) status |= CP_QP_SINGULAR;
+            if (inactive_slip_removal(n, PA, b, A, x_beta_old, x_beta, &rounds, &maxcond)) status |= CP_QP_SINGULAR;
             rounds_total += rounds;
             nPA = (int)PA.size();
             del_FP = zero3();
@@ -1062,6 +1073,7 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
     if (flag == 1 && io.dPdF)
         for (int i = 0; i < 81; ++i) finite &= std::isfinite(io.dPdF[i]);
     if (!finite) status |= CP_QP_NONFINITE;
+    if (maxcond > 1e12) status |= CP_QP_ILL_CONDITIONED;
     if (io.stats) {
         io.stats[0] = p0 < 0 ? 0 : p0;
         io.stats[1] = nPA;
@@ -1070,8 +1082,9 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
         io.stats[4] = c_terms;
         io.stats[5] = (int)iter1;
         io.stats[6] = 0;
-        io.stats[7] = status;
+        io.stats[7] = std::isfinite(maxcond) ? std::min(99, (int)std::ceil(std::log10(maxcond))) : 99;
     }
+    if (io.status) *io.status = status;
     return status;
 }
 
@@ -1091,7 +1104,7 @@ extern "C" {
 
 int oracle_update(const cp_material_t* mat, const cp_options_t* opt, const or_state* st,
                   const double* F, int32_t flag, double F_e, double F_r, double* P, double* T,
-                  double* dPdF, int32_t* stats, int32_t nthreads) {
+                  double* dPdF, int32_t* stats, int32_t* status, int32_t nthreads) {
     if (!mat || !opt || !st || !F) return CP_E_ARG;
     const Lattice L = make_lattice(mat);
     if (L.n <= 0 || L.n > NM) return CP_E_ARG;
@@ -1105,6 +1118,7 @@ int oracle_update(const cp_material_t* mat, const cp_options_t* opt, const or_st
         io.T = T ? T + 9 * k : nullptr;
         io.dPdF = (dPdF && flag == 1) ? dPdF + 81 * k : nullptr;
         io.stats = stats ? stats + 8 * k : nullptr;
+        io.status = status ? status + k : nullptr;
         bad |= calculate_plasticity(L, *opt, *st, k, io, flag, F_e, F_r);
     }
     return bad & (CP_QP_NONFINITE | CP_QP_SINGULAR) ? 1 : 0;
@@ -1113,7 +1127,7 @@ int oracle_update(const cp_material_t* mat, const cp_options_t* opt, const or_st
 int oracle_assemble(const cp_material_t* mat, const cp_options_t* opt, const or_state* st,
                     int64_t n_cells, const double* U, const double* gradN, const double* JxW,
                     int32_t uniform, double F_e, double F_r, double* Ke, double* Re, int32_t* stats,
-                    int32_t nthreads) {
+                    int32_t* status, int32_t nthreads) {
     if (!mat || !opt || !st || !U || !gradN || !JxW || !Ke || !Re) return CP_E_ARG;
     if (st->n_qp != 8 * n_cells) return CP_E_ARG;
     const Lattice L = make_lattice(mat);
@@ -1138,7 +1152,7 @@ int oracle_assemble(const cp_material_t* mat, const cp_options_t* opt, const or_
             }
             for (int i = 0; i < 3; ++i) F[4 * i] += 1;
             const int64_t k = 8 * c + q;
-            QpIO io{F, P, nullptr, dPdF, stats ? stats + 8 * k : nullptr};
+            QpIO io{F, P, nullptr, dPdF, stats ? stats + 8 * k : nullptr, status ? status + k : nullptr};
             bad |= calculate_plasticity(L, *opt, *st, k, io, 1, F_e, F_r);
             for (int d = 0; d < 24; ++d) {
                 const int i = d % 3;
@@ -1237,7 +1251,7 @@ int oracle_matrix_exponential(const double A[9], double out[9]) {
     return terms;
 }
 
-int oracle_pinv_svd(const double* A, int n, double* Ainv) { return pinv_svd(A, n, Ainv); }
+int oracle_pinv_svd(const double* A, int n, double* Ainv) { return pinv_svd(A, n, Ainv, nullptr); }
 
 int oracle_invert(const double* A, int n, double* Ainv) { return invert_n(A, n, Ainv); }
 

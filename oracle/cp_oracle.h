@@ -40,11 +40,12 @@ typedef struct or_state {
 } or_state;
 
 /* calculatePlasticity for qps [0, n_qp): F 9*n_qp; P,T 9*n_qp (nullable);
- * dPdF 81*n_qp when flag==1 (nullable); stats 8*n_qp (nullable). */
+ * dPdF 81*n_qp when flag==1 (nullable); stats 8*n_qp and status n_qp
+ * (nullable; same layouts as cp_get_stats / cp_update). */
 int oracle_update(const cp_material_t* mat, const cp_options_t* opt,
                   const or_state* st, const double* F, int32_t flag,
                   double F_e, double F_r, double* P, double* T, double* dPdF,
-                  int32_t* stats, int32_t nthreads);
+                  int32_t* stats, int32_t* status, int32_t nthreads);
 
 /* getElementalValues for n_cells cells (qp k = 8*cell+q).  gradN: per cell
  * 8*8*3 (or shared when uniform), JxW per cell 8 (or shared).  Writes Ke
@@ -53,7 +54,7 @@ int oracle_assemble(const cp_material_t* mat, const cp_options_t* opt,
                     const or_state* st, int64_t n_cells, const double* U,
                     const double* gradN, const double* JxW, int32_t uniform,
                     double F_e, double F_r, double* Ke, double* Re,
-                    int32_t* stats, int32_t nthreads);
+                    int32_t* stats, int32_t* status, int32_t nthreads);
 
 /* rotnew_conv = rotnew_iter; reorient(); rotnew_iter = rotnew_conv
  * (updateAfterIncrement.cc:287-295, reorient.cc:18-96). */

@@ -50,9 +50,9 @@ def lib() -> C.CDLL:
     if _lib is None:
         L = C.CDLL(build())
         M, O, S = C.POINTER(CpMaterial), C.POINTER(CpOptions), C.POINTER(OrState)
-        L.oracle_update.argtypes = [M, O, S, D, C.c_int32, C.c_double, C.c_double, D, D, D, I32, C.c_int32]
+        L.oracle_update.argtypes = [M, O, S, D, C.c_int32, C.c_double, C.c_double, D, D, D, I32, I32, C.c_int32]
         L.oracle_assemble.argtypes = [M, O, S, C.c_int64, D, D, D, C.c_int32, C.c_double, C.c_double,
-                                      D, D, I32, C.c_int32]
+                                      D, D, I32, I32, C.c_int32]
         L.oracle_reorient.argtypes = [S, C.c_int32]
         L.oracle_odfpoint.argtypes = [D, D]
         L.oracle_elasticmoduli.argtypes = [D, D, D]
@@ -170,7 +170,9 @@ class OracleBackend:
         for L, mat in enumerate(self.lattices):
             idx = np.nonzero(lid == L)[0]
             if len(idx):
-                self.groups.append(_Group(mat, idx, rod[idx]))
+                g = _Group(mat, idx, rod[idx])
+                g.lattice = L
+                self.groups.append(g)
 
     def update(self, F, flag, F_e=0.0, F_r=0.0, want_T=True):
         F = np.ascontiguousarray(F, float).reshape(self.n_qp, 9)
@@ -178,22 +180,27 @@ class OracleBackend:
         T = np.empty((self.n_qp, 9))
         dPdF = np.empty((self.n_qp, 81)) if flag == 1 else None
         stats = np.zeros((self.n_qp, 8), dtype=np.int32)
-        for g in self.groups:
+        status = np.zeros(self.n_qp, dtype=np.int32)
+        for L, g in self._lattice_groups():
             m = len(g.idx)
             Fg = np.ascontiguousarray(F[g.idx])
             Pg, Tg = np.empty((m, 9)), np.empty((m, 9))
             dg = np.empty((m, 81)) if flag == 1 else None
             sg = np.zeros((m, 8), dtype=np.int32)
+            qs = np.zeros(m, dtype=np.int32)
             lib().oracle_update(C.byref(g.mat), C.byref(self.options), C.byref(g.st), _p(Fg), flag,
-                                F_e, F_r, _p(Pg), _p(Tg), _p(dg), _pi(sg), self.nthreads)
+                                F_e, F_r, _p(Pg), _p(Tg), _p(dg), _pi(sg), _pi(qs), self.nthreads)
             P[g.idx], T[g.idx] = Pg, Tg
             if flag == 1:
                 dPdF[g.idx] = dg
-            sg[:, 6] = self.lattices.index(g.mat) if g.mat in self.lattices else 0
+            sg[:, 6] = L
             stats[g.idx] = sg
+            status[g.idx] = qs
         self.last_F, self.last_T, self.last_stats = F, T, stats
-        status = stats[:, 7].copy()
         return P, T, dPdF, status
+
+    def _lattice_groups(self):
+        return [(g.lattice, g) for g in self.groups]
 
     def stats(self):
         return self.last_stats
@@ -217,8 +224,8 @@ class OracleBackend:
         Re = np.empty((self.n_cells, 24))
         cl = self._cell_groups()
         stats = np.zeros((self.n_qp, 8), dtype=np.int32)
-        for g in self.groups:
-            L = self.lattices.index(g.mat)
+        status = np.zeros(self.n_qp, dtype=np.int32)
+        for L, g in self._lattice_groups():
             cells = np.nonzero(cl == L)[0]
             # group qps are ordered like the caller's qps, so cell-major order holds
             assert np.array_equal(g.idx, (8 * cells[:, None] + np.arange(8)).ravel())
@@ -229,13 +236,16 @@ class OracleBackend:
             Kg = np.empty((len(cells), 24, 24))
             Rg = np.empty((len(cells), 24))
             sg = np.zeros((len(g.idx), 8), dtype=np.int32)
+            qs = np.zeros(len(g.idx), dtype=np.int32)
             lib().oracle_assemble(C.byref(g.mat), C.byref(self.options), C.byref(g.st), len(cells),
                                   _p(Ug), _p(gN), _p(w), 1 if self.uniform else 0, F_e, F_r,
-                                  _p(Kg), _p(Rg), _pi(sg), self.nthreads)
+                                  _p(Kg), _p(Rg), _pi(sg), _pi(qs), self.nthreads)
             Ke[cells], Re[cells] = Kg, Rg
+            sg[:, 6] = L
             stats[g.idx] = sg
+            status[g.idx] = qs
         self.last_stats = stats
-        return Ke, Re, stats[:, 7].copy()
+        return Ke, Re, status
 
     def averages(self):
         """updateAfterIncrement.cc:119-126,218-235,710-722 over the last update."""

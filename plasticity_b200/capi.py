@@ -29,6 +29,7 @@ CP_QP_SINGULAR = 2
 CP_QP_ACTIVE_OVERFLOW = 4
 CP_QP_SERIES_CAP = 8
 CP_QP_SLIP_SEARCH_CAP = 16
+CP_QP_ILL_CONDITIONED = 32
 CP_QP_ERROR_MASK = CP_QP_NONFINITE | CP_QP_SINGULAR | CP_QP_ACTIVE_OVERFLOW | CP_QP_SERIES_CAP
 
 FIELDS = {

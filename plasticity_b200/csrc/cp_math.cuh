@@ -6,9 +6,29 @@
 // and vecform/matform of matrixOperations.cc:133-163 (Voigt 11,22,33,23,13,12).
 #pragma once
 
+#ifdef __CUDACC__
 #include <cuda_runtime.h>
-
 #define CP_HD __host__ __device__ __forceinline__
+#else
+// host-only compilation of the kernel sources (tests build them with g++ to
+// check the device code path against the oracle without a GPU)
+#include <cmath>
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#define __restrict__
+#define CP_HD inline
+using std::fabs;
+using std::fmax;
+using std::fmin;
+using std::ceil;
+using std::log10;
+using std::isfinite;
+using std::pow;
+using std::sqrt;
+using std::cos;
+using std::atan;
+#endif
 
 namespace cp {
 

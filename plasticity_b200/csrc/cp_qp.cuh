@@ -39,7 +39,7 @@ constexpr int GATEAUX_TERM_CAP = 64;  // count3 terms
 
 // status bits (include/cp_gpu.h)
 constexpr int QP_NONFINITE = 1, QP_SINGULAR = 2, QP_ACTIVE_OVERFLOW = 4, QP_SERIES_CAP = 8,
-              QP_SLIP_SEARCH_CAP = 16;
+              QP_SLIP_SEARCH_CAP = 16, QP_ILL_CONDITIONED = 32;
 
 // Per-lattice constants, one copy in global memory per lattice.
 struct LatDev {
@@ -74,21 +74,27 @@ struct QpOut {
     double scale;  // multiplies P and dPdF (JxW in the fused assembly, else 1)
 };
 
-__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+__host__ __device__ __forceinline__ double ldg(const double* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
 
-__device__ __forceinline__ M3 load_soa3(const double* __restrict__ f, int64_t cnt, int64_t i) {
+__host__ __device__ __forceinline__ M3 load_soa3(const double* __restrict__ f, int64_t cnt, int64_t i) {
     M3 m;
 #pragma unroll
     for (int c = 0; c < 9; ++c) m.a[c] = f[c * cnt + i];
     return m;
 }
-__device__ __forceinline__ void store_soa3(double* __restrict__ f, int64_t cnt, int64_t i, const M3& m) {
+__host__ __device__ __forceinline__ void store_soa3(double* __restrict__ f, int64_t cnt, int64_t i, const M3& m) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) f[c * cnt + i] = m.a[c];
 }
 
 // resolved shear m . (R^T X R) . n in the crystal frame
-__device__ __forceinline__ double resolved(const LatDev& L, int s, const M3& Xc) {
+__host__ __device__ __forceinline__ double resolved(const LatDev& L, int s, const M3& Xc) {
     const double m0 = ldg(&L.m[3 * s]), m1 = ldg(&L.m[3 * s + 1]), m2 = ldg(&L.m[3 * s + 2]);
     const double n0 = ldg(&L.nn[3 * s]), n1 = ldg(&L.nn[3 * s + 1]), n2 = ldg(&L.nn[3 * s + 2]);
     const double y0 = Xc(0, 0) * n0 + Xc(0, 1) * n1 + Xc(0, 2) * n2;
@@ -98,7 +104,7 @@ __device__ __forceinline__ double resolved(const LatDev& L, int s, const M3& Xc)
 }
 
 // sample-frame Schmid tensor S = (R m)(R n)^T
-__device__ __forceinline__ M3 schmid(const LatDev& L, int s, const M3& R) {
+__host__ __device__ __forceinline__ M3 schmid(const LatDev& L, int s, const M3& R) {
     double rm[3], rn[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -114,7 +120,7 @@ __device__ __forceinline__ M3 schmid(const LatDev& L, int s, const M3& R) {
 }
 
 // matrixExponential (matrixOperations.cc:165-186)
-__device__ __forceinline__ M3 matexp(const M3& A, int* terms, int* status) {
+__host__ __device__ __forceinline__ M3 matexp(const M3& A, int* terms, int* status) {
     M3 E = eye3(), t = eye3();
     double count = 1.0;
     int k = 0;
@@ -135,9 +141,13 @@ __device__ __forceinline__ M3 matexp(const M3& A, int* terms, int* status) {
 
 // In-place LU with partial pivoting of a row-major m x m block (leading
 // dimension ld) and solve for nrhs right-hand sides stored row-major (m x
-// nrhs, leading dimension ldb).  Returns nonzero on a zero pivot.
-__device__ __forceinline__ int lu_solve(double* A, int m, int ld, double* B, int nrhs, int ldb) {
+// nrhs, leading dimension ldb).  Returns nonzero on a zero pivot.  *cond
+// (optional) receives max|u_jj| / min|u_jj|, a cheap estimate of the
+// condition number used to flag numerically singular active-set blocks.
+__host__ __device__ __forceinline__ int lu_solve(double* A, int m, int ld, double* B, int nrhs, int ldb,
+                                                 double* cond = nullptr) {
     int sing = 0;
+    double pmin = 1e308, pmax = 0.0;
     for (int j = 0; j < m; ++j) {
         int r = j;
         double mx = fabs(A[j * ld + j]);
@@ -148,6 +158,8 @@ __device__ __forceinline__ int lu_solve(double* A, int m, int ld, double* B, int
                 r = i;
             }
         }
+        pmin = fmin(pmin, mx);
+        pmax = fmax(pmax, mx);
         if (mx == 0.0) {
             sing = 1;
             continue;
@@ -180,12 +192,13 @@ __device__ __forceinline__ int lu_solve(double* A, int m, int ld, double* B, int
             B[j * ldb + c] = s / d;
         }
     }
+    if (cond) *cond = m == 0 ? 1.0 : (pmin > 0.0 ? pmax / pmin : 1e308);
     return sing;
 }
 
 // D_k recurrence for the Gateaux series; returns S + sum_k cm(k) D_k and
 // S + sum_k cp(k) D_k with cm(k) = (-1)^k/(k+1)!, cp(k) = 1/(k+1)!.
-__device__ __forceinline__ void gateaux_pair(const M3& S, const M3& P, int count3, M3& dminus, M3& dplus) {
+__host__ __device__ __forceinline__ void gateaux_pair(const M3& S, const M3& P, int count3, M3& dminus, M3& dplus) {
     dminus = S;
     dplus = S;
     M3 D = S, Pk = eye3();
@@ -216,7 +229,7 @@ struct QpScratch {
 
 // The whole calculatePlasticity for internal qp i of group g.
 template <int NT, int PMAX>
-__device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
+__host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
                          double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id) {
     QpScratch<NT, PMAX> w;
     const int n = L.n, ns = L.ns, nw = L.nw;
@@ -248,6 +261,7 @@ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int6
     double dFp[81];
     bool dFp_nonzero = false;
     int nPA = 0, p0 = -1, rounds_total = 0, e_terms = 0, c_terms = 0;
+    double maxcond = 1.0;
     int iter1 = 1;
 
     while (true) {
@@ -362,7 +376,9 @@ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int6
                     w.rhs[r] = w.b[w.pa0[kr]];
                     for (int c = 0; c < m; ++c) w.Apa[r * PMAX + c] = w.A[kr * PMAX + w.pa[c]];
                 }
-                if (lu_solve(w.Apa, m, PMAX, w.rhs, 1, 1)) status |= QP_SINGULAR;
+                double cnd = 1.0;
+                if (lu_solve(w.Apa, m, PMAX, w.rhs, 1, 1, &cnd)) status |= QP_SINGULAR;
+                maxcond = fmax(maxcond, cnd);
                 ++rounds_total;
                 for (int k = 0; k < p_init; ++k) w.x[k] = 0.0;
                 for (int r = 0; r < m; ++r) w.x[w.pa[r]] = w.rhs[r];
@@ -686,6 +702,7 @@ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int6
 #pragma unroll
     for (int c = 0; c < 9; ++c) finite = finite && isfinite(P_tau.a[c]);
     if (!finite) status |= QP_NONFINITE;
+    if (maxcond > 1e12) status |= QP_ILL_CONDITIONED;
     if (stats_out) {
         stats_out[0] = p0 < 0 ? 0 : p0;
         stats_out[1] = nPA;
@@ -694,7 +711,7 @@ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev& g, int6
         stats_out[4] = c_terms;
         stats_out[5] = iter1;
         stats_out[6] = lattice_id;
-        stats_out[7] = status;
+        stats_out[7] = maxcond >= 1e99 ? 99 : (int)ceil(log10(maxcond));
     }
     return status;
 }

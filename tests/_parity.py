@@ -6,6 +6,7 @@ import numpy as np
 from plasticity_b200 import materials as M
 
 TOL = 1e-10  # FP64 parity bar for stresses, tangents and history (relative, per qp)
+COND_MAX_EXP = 12  # active-set solves with condition > 1e12 are ill-posed (see well_posed)
 
 STATE_FIELDS = ["Fp", "Fe", "s", "W", "rot", "rotnew", "twinfrac", "slipfrac", "twin"]
 
@@ -54,3 +55,16 @@ def make_pair(oracle_lib, mats, lattice_id, seed, steps, opts=None, amp=2e-4):
     gh.bind_qps(lattice_id, rod)
     copy_state(ob, gh)
     return gh, ob, F, rng
+
+
+def well_posed(*stats):
+    """qps whose active-set solves were well conditioned (condition <= 1e12)
+    on every side compared.  Above that, the reference's
+    compute_inverse_svd(0.0) solution is set by rounding noise (A_PA is
+    numerically singular: for FCC both the latent-hardening part and the
+    Schmid part of A have rank <= 5), so no two implementations agree; those
+    qps are flagged CP_QP_ILL_CONDITIONED and counted instead."""
+    m = np.ones(len(stats[0]), dtype=bool)
+    for s in stats:
+        m &= np.asarray(s)[:, 7] <= COND_MAX_EXP
+    return m
