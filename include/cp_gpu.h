@@ -197,6 +197,32 @@ int cp_assemble_device(cp_handle* h, const double* d_U_local, double F_e,
  */
 int cp_averages(cp_handle* h, double out[22]);
 
+/*
+ * cp_averages without any device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: host codes whose device memory is
+ * handed to their own pool allocator up front (a PETSc/Kokkos-style pool in
+ * the FE application owns the GPU's memory), and per-increment callbacks that
+ * must not pay cudaMalloc/cudaFree, which synchronise the whole device and
+ * stall the caller's other streams.  cp_averages allocates its reduction
+ * scratch on first use; this variant instead uses a file-scope device array
+ * compiled into the library (about 2.9 MB, held on every GPU that loads the
+ * library until the process exits) and calls no allocating routine.
+ *
+ * Same inputs, outputs and summation order as cp_averages.  Limits and rules:
+ *   - at most CP_NOALLOC_AVG_MAX_QPS bound qps; larger handles get CP_E_ARG
+ *     with a message naming the limit;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) for that device; make that first call before
+ *     any stream capture;
+ *   - every call on a device shares the one array and it keeps the last
+ *     call's contents (each call writes every entry it reads, so nothing
+ *     needs clearing); calls that overlap on the GPU (different handles on
+ *     different streams of the same device) race on it.
+ */
+#define CP_NOALLOC_AVG_MAX_QPS (1 << 22)
+int cp_averages_noalloc(cp_handle* h, double out[22]);
+
 /* reorient() (reorient.cc:4-98) on all qps: updates rotnew_conv. */
 int cp_reorient(cp_handle* h);
 

@@ -154,6 +154,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_assemble_device": (C.c_int, [H, C.c_void_p, C.c_double, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
         "cp_averages": (C.c_int, [H, D]),
+        "cp_averages_noalloc": (C.c_int, [H, D]),
         "cp_reorient": (C.c_int, [H]),
         "cp_commit": (C.c_int, [H]),
         "cp_field_width": (C.c_int32, [H, C.c_int32]),

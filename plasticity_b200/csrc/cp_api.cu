@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -244,6 +245,14 @@ __global__ void fp64_fma_probe_kernel(int iters, double seed, double* out) {
 }
 
 }  // namespace cp
+
+// ---------------------------------------------------------------- no-alloc averages scratch
+// Device-resident scratch for cp_averages_noalloc: one row of AVG_N partial
+// sums per reduction block (up to CP_NOALLOC_AVG_MAX_QPS qps, plus one spare
+// block per lattice group for the per-group rounding) and one final row.
+// Every GPU that loads this library holds it (about 2.9 MB) until exit.
+constexpr int64_t NOALLOC_AVG_BLOCKS = CP_NOALLOC_AVG_MAX_QPS / cp::AVG_BLOCK + CP_MAX_LATTICES;
+static __device__ __align__(256) double g_noalloc_avg_scratch[(NOALLOC_AVG_BLOCKS + 1) * cp::AVG_N];
 
 // ---------------------------------------------------------------- handle
 namespace {
@@ -786,6 +795,63 @@ int cp_averages(cp_handle* h, double out[22]) {
     CK(h, cudaGetLastError());
     double sums[AVG_N];
     CK(h, cudaMemcpyAsync(sums, h->d_avg_out, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    const double vol = sums[21];
+    for (int c = 0; c < 21; ++c) out[c] = sums[c] / vol;
+    out[21] = vol;
+    return CP_OK;
+}
+
+// Device address of g_noalloc_avg_scratch, looked up once per device (the
+// symbol's host-side name is a stand-in, not a device address).
+static double* noalloc_avg_scratch(int device, cudaError_t* err) {
+    static std::mutex mu;
+    static double* addr[64] = {nullptr};
+    *err = cudaSuccess;
+    if (device < 0 || device >= 64) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        *err = cudaGetSymbolAddress(&p, g_noalloc_avg_scratch);
+        if (*err != cudaSuccess) return nullptr;
+        addr[device] = static_cast<double*>(p);
+    }
+    return addr[device];
+}
+
+int cp_averages_noalloc(cp_handle* h, double out[22]) {
+    if (!h || !out) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_averages_noalloc: no mesh bound (JxW needed)");
+    if (!h->have_post) return fail(h, CP_E_STATE, "cp_averages_noalloc: no cp_update with stiffness_flag 0 yet");
+    if (h->n_qp > (int64_t)CP_NOALLOC_AVG_MAX_QPS)
+        return fail(h, CP_E_ARG, "cp_averages_noalloc: " + std::to_string(h->n_qp) +
+                                     " qps exceed the static scratch limit CP_NOALLOC_AVG_MAX_QPS (" +
+                                     std::to_string((int64_t)CP_NOALLOC_AVG_MAX_QPS) + "); use cp_averages");
+    if (int rc = check_device(h)) return rc;
+    int64_t nblocks = 0;
+    for (const auto& g : h->groups) nblocks += blocks_for(g.count, AVG_BLOCK);
+    if (nblocks > NOALLOC_AVG_BLOCKS) return fail(h, CP_E_ARG, "cp_averages_noalloc: scratch too small");
+    cudaError_t e;
+    double* scratch = noalloc_avg_scratch(h->device, &e);
+    if (!scratch) return cuda_fail(h, e, "cp_averages_noalloc: cudaGetSymbolAddress");
+    double* partial = scratch;
+    double* final_row = scratch + NOALLOC_AVG_BLOCKS * AVG_N;
+    // every partial row read below is written earlier in this call, so the
+    // scratch needs no clearing between calls
+    int64_t off = 0;
+    for (const auto& g : h->groups) {
+        const unsigned nb = blocks_for(g.count, AVG_BLOCK);
+        averages_partial_kernel<<<nb, AVG_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], g.dev, h->d_keepF, h->d_keepT,
+                                                                 h->d_JxW, h->uniform, partial + off * AVG_N);
+        off += nb;
+    }
+    averages_final_kernel<<<1, 32, 0, h->stream>>>(partial, (int)nblocks, final_row);
+    CK(h, cudaGetLastError());
+    double sums[AVG_N];
+    CK(h, cudaMemcpyAsync(sums, final_row, sizeof sums, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
     const double vol = sums[21];
     for (int c = 0; c < 21; ++c) out[c] = sums[c] / vol;
