@@ -99,8 +99,12 @@ typedef struct cp_options_t {
     int32_t max_solver_iterations;      /* modelMaxSolverIterations */
     int32_t enable_multiphase;          /* F_T rule, calculatePlasticity.cc:970-980 */
     int32_t device;                     /* CUDA device ordinal */
-    int32_t block_size;                 /* threads per block for the qp kernels (0 = autotuned) */
-    int32_t use_graphs;                 /* capture repeated launches in CUDA graphs (1) */
+    int32_t block_size;                 /* reserved (0) */
+    int32_t use_graphs;                 /* reserved (0) */
+    int32_t plain_kernel;               /* 1: one thread per qp in bind order with full-size per-thread
+                                           scratch (the plain FP64 drop-in, kept as a baseline);
+                                           0 (default): qps sorted by potentially-active-set size each
+                                           call, compact per-thread scratch */
 } cp_options_t;
 
 typedef struct cp_handle cp_handle;

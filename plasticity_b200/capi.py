@@ -80,6 +80,7 @@ class CpOptions(C.Structure):
         ("device", C.c_int32),
         ("block_size", C.c_int32),
         ("use_graphs", C.c_int32),
+        ("plain_kernel", C.c_int32),
     ]
 
 
@@ -92,7 +93,8 @@ def default_options(**kw) -> CpOptions:
     o.enable_multiphase = 0
     o.device = 0
     o.block_size = 0
-    o.use_graphs = 1
+    o.use_graphs = 0
+    o.plain_kernel = 0
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -265,6 +265,9 @@ struct Group {
     int64_t* d_qp = nullptr;
     double* d_block = nullptr;  // one allocation for all double fields
     int* d_twin = nullptr;      // twin_c, twin_i
+    unsigned char* d_key = nullptr;  // sort key per internal qp
+    int* d_perm = nullptr;           // internal qps in sorted order
+    int* d_hist = nullptr;           // SORT_BUCKETS counts, then SORT_BUCKETS offsets
     GroupDev dev{};
 };
 
@@ -294,6 +297,7 @@ struct cp_handle {
     int uniform = 1;
     double *d_gradN = nullptr, *d_JxW = nullptr;
     double *d_U = nullptr, *d_Ke = nullptr, *d_Re = nullptr;
+    double* d_stage = nullptr;  // JxW*P and JxW*dP/dF per qp between update and contraction
     // averages scratch
     double *d_avg_partial = nullptr, *d_avg_out = nullptr;
     int64_t avg_cap = 0;
@@ -332,6 +336,9 @@ void free_group(Group& g) {
     cudaFree(g.d_qp);
     cudaFree(g.d_block);
     cudaFree(g.d_twin);
+    cudaFree(g.d_key);
+    cudaFree(g.d_perm);
+    cudaFree(g.d_hist);
     g = Group{};
 }
 
@@ -361,7 +368,8 @@ void free_mesh(cp_handle* h) {
     cudaFree(h->d_U);
     cudaFree(h->d_Ke);
     cudaFree(h->d_Re);
-    h->d_gradN = h->d_JxW = h->d_U = h->d_Ke = h->d_Re = nullptr;
+    cudaFree(h->d_stage);
+    h->d_gradN = h->d_JxW = h->d_U = h->d_Ke = h->d_Re = h->d_stage = nullptr;
     h->n_cells = 0;
 }
 
@@ -437,8 +445,51 @@ void timing_end(cp_handle* h, int gi, cudaEvent_t a) {
     h->pending.push_back({a, b, gi});
 }
 
+// sort the group's qps by potentially-active-set size (descending)
+template <class FSrc>
+void sort_group(cp_handle* h, const Group& g, FSrc fs) {
+    cudaMemsetAsync(g.d_hist, 0, sizeof(int) * SORT_BUCKETS, h->stream);
+    classify_kernel<FSrc><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], h->dopts,
+                                                                                   g.dev, fs, g.d_key, g.d_hist);
+    bucket_scan_kernel<<<1, 32, 0, h->stream>>>(g.d_hist, g.d_hist + SORT_BUCKETS);
+    bucket_scatter_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(g.d_key, g.count, g.d_hist + SORT_BUCKETS,
+                                                                         g.d_perm);
+}
+
+template <int PMAX, class FSrc>
+void launch_update2(cp_handle* h, const Group& g, FSrc fs, int flag, double F_e, double F_r, double* P, double* T,
+                    double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
+    update2_kernel<PMAX, FSrc><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(
+        h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats, kF, kT,
+        g.lattice);
+}
+
+template <class FSrc>
+void sorted_update_group(cp_handle* h, size_t gi, FSrc fs, int flag, double F_e, double F_r, double* P, double* T,
+                         double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
+    const Group& g = h->groups[gi];
+    sort_group(h, g, fs);
+    cudaEvent_t ev{};
+    timing_begin(h, (int)gi, &ev);
+    switch (g.nt_class) {
+        case 16: launch_update2<16>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+        case 32: launch_update2<32>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+        default: launch_update2<48>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+    }
+    timing_end(h, (int)gi, ev);
+}
+
 int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double F_r, double* P, double* T,
                     double* dPdF, int32_t* st) {
+    if (!h->opts.plain_kernel) {
+        double* kF = flag == 0 ? h->d_keepF : nullptr;
+        double* kT = flag == 0 ? h->d_keepT : nullptr;
+        for (size_t gi = 0; gi < h->groups.size(); ++gi)
+            sorted_update_group(h, gi, FromArray{F}, flag, F_e, F_r, P, T, dPdF, nullptr, st, kF, kT);
+        CK(h, cudaGetLastError());
+        if (flag == 0) h->have_post = true;
+        return CP_OK;
+    }
     double* kF = flag == 0 ? h->d_keepF : nullptr;
     double* kT = flag == 0 ? h->d_keepT : nullptr;
     for (size_t gi = 0; gi < h->groups.size(); ++gi) {
@@ -619,7 +670,10 @@ int cp_bind_qps(cp_handle* h, int64_t n_qp, const int32_t* lattice_id, const dou
         g.count = (int64_t)idx[l].size();
         if (cudaMalloc(&g.d_qp, sizeof(int64_t) * g.count) != cudaSuccess ||
             cudaMalloc(&g.d_block, sizeof(double) * group_doubles(g.n, g.ns, g.nw, g.count)) != cudaSuccess ||
-            cudaMalloc(&g.d_twin, sizeof(int) * 2 * g.count) != cudaSuccess) {
+            cudaMalloc(&g.d_twin, sizeof(int) * 2 * g.count) != cudaSuccess ||
+            cudaMalloc(&g.d_key, g.count) != cudaSuccess ||
+            cudaMalloc(&g.d_perm, sizeof(int) * g.count) != cudaSuccess ||
+            cudaMalloc(&g.d_hist, sizeof(int) * 2 * SORT_BUCKETS) != cudaSuccess) {
             free_group(g);
             cudaFree(d_rod);
             free_qps(h);
@@ -727,6 +781,18 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
     if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble: no mesh bound");
     if (!d_U || !d_Ke || !d_Re) return fail(h, CP_E_ARG, "cp_assemble: bad arguments");
     if (int rc = check_device(h)) return rc;
+    if (!h->opts.plain_kernel) {
+        if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "cp_assemble: staging allocation failed");
+        const FromMesh fm{d_U, h->d_gradN, h->d_JxW, h->uniform};
+        for (size_t gi = 0; gi < h->groups.size(); ++gi)
+            sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status, nullptr,
+                                nullptr);
+        contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
+            h->d_stage, h->d_gradN, h->uniform, h->n_cells, d_Ke, d_Re);
+        CK(h, cudaGetLastError());
+        return CP_OK;
+    }
     for (size_t gi = 0; gi < h->groups.size(); ++gi) {
         const auto& g = h->groups[gi];
         cudaEvent_t ev{};

@@ -1,7 +1,7 @@
 // cp_kernels.cuh -- the CUDA kernels behind include/cp_gpu.h.
 #pragma once
 
-#include "cp_qp.cuh"
+#include "cp_qp2.cuh"
 
 namespace cp {
 
@@ -112,6 +112,192 @@ __global__ void __launch_bounds__(QP_BLOCK) assemble_kernel(const LatDev* __rest
 #pragma unroll
             for (int cj = 0; cj < 3; ++cj) {
                 // t_l = sum_k g1_k dPdF[ci][k][cj][l]
+                double t[3];
+#pragma unroll
+                for (int l = 0; l < 3; ++l)
+                    t[l] = g1x * Dq[27 * ci + 0 + 3 * cj + l] + g1y * Dq[27 * ci + 9 + 3 * cj + l] +
+                           g1z * Dq[27 * ci + 18 + 3 * cj + l];
+#pragma unroll
+                for (int a2 = 0; a2 < 8; ++a2)
+                    K[ci][3 * a2 + cj] += t[0] * gq[a2 * 3] + t[1] * gq[a2 * 3 + 1] + t[2] * gq[a2 * 3 + 2];
+            }
+        }
+    }
+    double* Kc = Ke + cell * 576 + (3 * a1) * 24;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 24; ++c) Kc[r * 24 + c] = K[r][c];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) Re[cell * 24 + 3 * a1 + r] = Rl[r];
+}
+
+// ---------------------------------------------------------------- sorted pipeline
+// F of caller qp k from a caller array ...
+struct FromArray {
+    const double* __restrict__ F;
+    __device__ __forceinline__ M3 operator()(int64_t k) const {
+        M3 m;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) m.a[c] = F[9 * k + c];
+        return m;
+    }
+    __device__ __forceinline__ double weight(int64_t) const { return 1.0; }
+};
+// ... or from the cell's nodal displacements (getElementalValues.cc:129-138):
+// qp k is Gauss point k % 8 of cell k / 8
+struct FromMesh {
+    const double* __restrict__ U;
+    const double* __restrict__ gradN;
+    const double* __restrict__ JxW;
+    int uniform;
+    __device__ __forceinline__ M3 operator()(int64_t k) const {
+        const int64_t cell = k >> 3;
+        const int q = (int)(k & 7);
+        const double* gq = (uniform ? gradN : gradN + cell * 192) + q * 24;
+        const double* Uc = U + 24 * cell;
+        M3 F = zero3();
+        for (int d = 0; d < 24; ++d) {
+            const int ci = d % 3, a = d / 3;
+            const double ud = Uc[d];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) F(ci, j) += ud * gq[a * 3 + j];
+        }
+        F(0, 0) += 1.0;
+        F(1, 1) += 1.0;
+        F(2, 2) += 1.0;
+        return F;
+    }
+    __device__ __forceinline__ double weight(int64_t k) const { return uniform ? JxW[k & 7] : JxW[k]; }
+};
+
+constexpr int SORT_BUCKETS = 64;
+
+// sort key: bucket 63 - min(p0, 63), so ascending buckets = descending p0
+template <class FSrc>
+__global__ void __launch_bounds__(QP_BLOCK) classify_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs,
+                                                            unsigned char* __restrict__ key, int* __restrict__ hist) {
+    __shared__ int sh[SORT_BUCKETS];
+    if (threadIdx.x < SORT_BUCKETS) sh[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.count) {
+        const int p0 = count_potentially_active(*L, o, g, i, fs(g.qp[i]));
+        const int b = SORT_BUCKETS - 1 - (p0 < SORT_BUCKETS - 1 ? p0 : SORT_BUCKETS - 1);
+        key[i] = (unsigned char)b;
+        atomicAdd(&sh[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < SORT_BUCKETS && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+// exclusive scan of the bucket counts (one warp, SORT_BUCKETS = 64)
+__global__ void bucket_scan_kernel(const int* __restrict__ hist, int* __restrict__ offs) {
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int b = 0; b < SORT_BUCKETS; ++b) {
+            offs[b] = acc;
+            acc += hist[b];
+        }
+    }
+}
+
+// scatter internal indices into bucket order (block-aggregated reservations)
+__global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char* __restrict__ key, int64_t count,
+                                                             int* __restrict__ offs, int* __restrict__ perm) {
+    __shared__ int cnt[SORT_BUCKETS], base[SORT_BUCKETS];
+    if (threadIdx.x < SORT_BUCKETS) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int b = 0, r = 0;
+    if (i < count) {
+        b = key[i];
+        r = atomicAdd(&cnt[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < SORT_BUCKETS) base[threadIdx.x] = cnt[threadIdx.x] ? atomicAdd(&offs[threadIdx.x], cnt[threadIdx.x]) : 0;
+    __syncthreads();
+    if (i < count) perm[base[b] + r] = (int)i;
+}
+
+// calculatePlasticity over one group in sorted order (thread j runs internal
+// qp perm[j]).  Outputs by caller index k: P/T/dPdF/status/stats; with a
+// non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
+template <int PMAX, class FSrc>
+__global__ void __launch_bounds__(QP_BLOCK) update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs,
+                                                           const int* __restrict__ perm, int flag, double F_e,
+                                                           double F_r, double* __restrict__ P, double* __restrict__ T,
+                                                           double* __restrict__ dPdF, double* __restrict__ stage,
+                                                           int32_t* __restrict__ status, int32_t* __restrict__ stats,
+                                                           double* __restrict__ keepF, double* __restrict__ keepT,
+                                                           int lattice_id) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.count) return;
+    const int64_t i = perm[j];
+    const int64_t k = g.qp[i];
+    const M3 F = fs(k);
+    double Tl[9];
+    QpOut out;
+    if (stage) {
+        out.P = stage + 90 * k;
+        out.dPdF = stage + 90 * k + 9;
+        out.scale = fs.weight(k);
+    } else {
+        out.P = P ? P + 9 * k : nullptr;
+        out.dPdF = (dPdF && flag == 1) ? dPdF + 81 * k : nullptr;
+        out.scale = 1.0;
+    }
+    out.T = (T || keepT) ? Tl : nullptr;
+    const int st = qp_update2<PMAX>(*L, o, g, i, F, flag, F_e, F_r, out, stats ? stats + 8 * k : nullptr, lattice_id);
+    if (T)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) T[9 * k + c] = Tl[c];
+    if (keepT) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            keepT[9 * k + c] = Tl[c];
+            keepF[9 * k + c] = F.a[c];
+        }
+    }
+    if (status) status[k] = st;
+}
+
+// Element contraction (getElementalValues.cc:144-162) from the staged JxW*P
+// and JxW*dP/dF of the cell's 8 qps: thread (cell, node a) writes rows
+// 3a..3a+2 of Ke and Re.  Cells are in caller order; CONTRACT_CELLS per block.
+constexpr int CONTRACT_CELLS = 8;
+__global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const double* __restrict__ stage,
+                                                                      const double* __restrict__ gradN, int uniform,
+                                                                      int64_t n_cells, double* __restrict__ Ke,
+                                                                      double* __restrict__ Re) {
+    __shared__ double sd[CONTRACT_CELLS][8 * 90];
+    const int tid = threadIdx.x;
+    const int lc = tid >> 3, a1 = tid & 7;
+    const int64_t cell0 = (int64_t)blockIdx.x * CONTRACT_CELLS;
+    // cooperative, coalesced load of the block's cells' staged values
+    const int64_t ncb = (n_cells - cell0) < CONTRACT_CELLS ? (n_cells - cell0) : CONTRACT_CELLS;
+    const double* src = stage + cell0 * 720;
+    for (int t = tid; t < ncb * 720; t += CONTRACT_CELLS * 8) sd[t / 720][t % 720] = src[t];
+    __syncthreads();
+    const int64_t cell = cell0 + lc;
+    if (cell >= n_cells) return;
+    const double* g0 = uniform ? gradN : gradN + cell * 192;
+    double K[3][24];
+    double Rl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 24; ++c) K[r][c] = 0.0;
+    for (int qq = 0; qq < 8; ++qq) {
+        const double* gq = g0 + qq * 24;
+        const double* Pq = &sd[lc][qq * 90];
+        const double* Dq = Pq + 9;
+        const double g1x = gq[a1 * 3], g1y = gq[a1 * 3 + 1], g1z = gq[a1 * 3 + 2];
+#pragma unroll
+        for (int ci = 0; ci < 3; ++ci) {
+            Rl[ci] -= g1x * Pq[3 * ci] + g1y * Pq[3 * ci + 1] + g1z * Pq[3 * ci + 2];
+#pragma unroll
+            for (int cj = 0; cj < 3; ++cj) {
                 double t[3];
 #pragma unroll
                 for (int l = 0; l < 3; ++l)

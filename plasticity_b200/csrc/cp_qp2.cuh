@@ -1,0 +1,534 @@
+// cp_qp2.cuh -- the per-qp constitutive update with compact per-thread state
+// (the optimised form of cp_qp.cuh's qp_update; same math, same order of the
+// reference's steps, see cp_qp.cuh's header for the restatements).
+//
+// Differences from the plain form, all about where intermediate values live:
+//   * no per-thread arrays over all n systems: the per-system loops read the
+//     history straight from the structure-of-arrays group (coalesced across a
+//     warp), and the _iter arrays of CRSS and backstress are the working
+//     storage of the current values (initialised from _conv on entry);
+//   * per-thread arrays are compact over the potentially active set of the
+//     current pass (capacity PMAX), and the consistency matrix is packed at its
+//     actual size, so the touched scratch grows with p0^2, not PMAX^2;
+//   * qps arrive sorted by potentially-active-set size (classify_kernel +
+//     counting sort), so the threads of a warp run solves of similar size.
+#pragma once
+
+#include "cp_qp.cuh"
+
+namespace cp {
+
+template <int PMAX>
+struct QpScratch2 {
+    unsigned char pa0[PMAX], cur[PMAX], pos[PMAX];
+    double tau_tr[PMAX], b[PMAX], h[PMAX], x_old[PMAX], x[PMAX], tn[PMAX];
+    double Spa[PMAX * 9];
+    double A[PMAX * PMAX];    // packed, leading dimension p_init
+    double Apa[PMAX * PMAX];  // packed, leading dimension m (or p for A2)
+    double rhs[PMAX * 9];
+};
+
+// Trial state of one slip-search pass (:160-196) and the potentially active
+// set count; shared by classify_kernel and qp_update2.
+struct Trial {
+    M3 Fpn_inv, CE, Tst, Xc;
+};
+
+__host__ __device__ __forceinline__ Trial trial_state(const M3& F, const M3& FP, const Sym6& D2, const M3& R) {
+    Trial t;
+    t.Fpn_inv = inv(FP);
+    const M3 FE = mul(F, t.Fpn_inv);
+    t.CE = mulTN(FE, FE);
+    M3 Ee = t.CE;
+    Ee(0, 0) -= 1.0;
+    Ee(1, 1) -= 1.0;
+    Ee(2, 2) -= 1.0;
+    Ee = scale(0.5, Ee);
+    t.Tst = voigt_apply(D2, Ee);
+    t.Xc = mulTN(R, mul(mul(t.CE, t.Tst), R));
+    return t;
+}
+
+// Potentially active systems at the increment start (first pass), the sort
+// key of the update.
+__host__ __device__ __forceinline__ int count_potentially_active(const LatDev& L, const Opts& o, const GroupDev& g,
+                                                                  int64_t i, const M3& F) {
+    const int64_t cnt = g.count;
+    const int n = L.n, ns = L.ns;
+    const M3 R = odfpoint(g.rot_c[i], g.rot_c[cnt + i], g.rot_c[2 * cnt + i]);
+    const Sym6 D2 = elasticmoduli(R, L.C);
+    const Trial t = trial_state(F, load_soa3(g.Fp_c, cnt, i), D2, R);
+    int p0 = 0;
+    for (int a = 0; a < n; ++a) {
+        const double W = g.W_c[(int64_t)a * cnt + i];
+        double tau = resolved(L, a, t.Xc);
+        if (a > ns - 1 && (tau - W) < 0) tau = W;
+        p0 += (fabs(tau - W) - g.s_c[(int64_t)a * cnt + i]) >= o.tol;
+    }
+    return p0;
+}
+
+template <int PMAX>
+__host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
+                                   double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id) {
+    QpScratch2<PMAX> w;
+    const int n = L.n, ns = L.ns, nw = L.nw;
+    const int64_t cnt = g.count;
+    int status = 0;
+    const double tol1 = o.tol;
+    double* __restrict__ s_cur = g.s_i;  // current CRSS of every system, [a * cnt + i]
+    double* __restrict__ W_cur = g.W_i;  // current backstress
+
+    // ---- history (:28-35): the _iter CRSS/backstress start as the _conv values
+    for (int a = 0; a < n; ++a) {
+        s_cur[(int64_t)a * cnt + i] = g.s_c[(int64_t)a * cnt + i];
+        W_cur[(int64_t)a * cnt + i] = g.W_c[(int64_t)a * cnt + i];
+    }
+    const double r0 = g.rot_c[i], r1 = g.rot_c[cnt + i], r2 = g.rot_c[2 * cnt + i];
+    const M3 R = odfpoint(r0, r1, r2);
+    const Sym6 D2 = elasticmoduli(R, L.C);
+
+    unsigned long long neg_t_bits = 0ull;
+    M3 FP_tau = load_soa3(g.Fp_c, cnt, i);
+    M3 Fpn_inv = inv(FP_tau);
+    M3 FE_tau = mul(F, Fpn_inv);
+    M3 FP_t2 = FP_tau, CE_tr = zero3(), Tst = zero3(), Ce_tau = zero3(), del_FP = zero3();
+    M3 T_tau, P_tau;
+    double dFp[81];
+    bool dFp_nonzero = false;
+    int nPA = 0, p0 = -1, rounds_total = 0, e_terms = 0, c_terms = 0;
+    double maxcond = 1.0;
+    int iter1 = 1;
+
+    while (true) {
+        if (iter1 > o.max_search) {
+            status |= QP_SLIP_SEARCH_CAP;
+            break;
+        }
+        // ---- trial kinematics and stress (:160-196)
+        FP_t2 = FP_tau;
+        const Trial tr = trial_state(F, FP_t2, D2, R);
+        Fpn_inv = tr.Fpn_inv;
+        CE_tr = tr.CE;
+        const M3 Tst_tr = tr.Tst;
+        Tst = Tst_tr;
+        {
+            const double dFe = det(FE_tau);
+            const M3 t = scale(1.0 / dFe, mul(FE_tau, Tst_tr));
+            T_tau = mulNT(t, FE_tau);
+            P_tau = scale(dFe, mulNT(T_tau, inv(F)));
+        }
+        // ---- resolved shears, potentially active set (:199-244), compact
+        nPA = 0;
+        for (int a = 0; a < n; ++a) {
+            const double W = W_cur[(int64_t)a * cnt + i];
+            double t = resolved(L, a, tr.Xc);
+            if (a > ns - 1 && (t - W) < 0) t = W;
+            const double bb = fabs(t - W) - s_cur[(int64_t)a * cnt + i];
+            if (bb >= tol1) {
+                if (nPA < PMAX) {
+                    w.pa0[nPA] = (unsigned char)a;
+                    w.tau_tr[nPA] = t;
+                    w.b[nPA] = bb;
+                } else {
+                    status |= QP_ACTIVE_OVERFLOW;
+                }
+                ++nPA;
+            }
+        }
+        if (nPA > PMAX) nPA = PMAX;
+        if (p0 < 0) p0 = nPA;
+        if (nPA == 0) break;
+        const int p_init = nPA;
+        neg_t_bits = 0ull;
+        for (int k = 0; k < p_init; ++k) {
+            const int a = w.pa0[k];
+            if ((w.tau_tr[k] - g.W_c[(int64_t)a * cnt + i]) < 0) neg_t_bits |= (1ull << a);
+        }
+
+        // ---- h_beta (:252-262) and A[PA,PA] (:265-306), packed p_init x p_init
+        for (int k = 0; k < p_init; ++k) {
+            const int a = w.pa0[k];
+            w.h[k] = ldg(&L.h0[a]) * pow((1 - s_cur[(int64_t)a * cnt + i] / ldg(&L.ss[a])), ldg(&L.a[a]));
+            const M3 S = schmid(L, a, R);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) w.Spa[k * 9 + c] = S.a[c];
+        }
+        for (int kj = 0; kj < p_init; ++kj) {
+            const int bsys = w.pa0[kj];
+            M3 Sj;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) Sj.a[c] = w.Spa[kj * 9 + c];
+            const M3 Y = sym(mul(CE_tr, Sj));
+            M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
+            axpy(Mj, 2.0, mul(Y, Tst_tr));
+            const double dj = w.tau_tr[kj] - W_cur[(int64_t)bsys * cnt + i];
+            for (int ki = 0; ki < p_init; ++ki) {
+                const int asys = w.pa0[ki];
+                M3 Si;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) Si.a[c] = w.Spa[ki * 9 + c];
+                const double Wa = W_cur[(int64_t)asys * cnt + i];
+                const double di = w.tau_tr[ki] - Wa;
+                const double sm = dot9(Si, Mj);
+                double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
+                v += (di * dj < 0.0) ? -sm : sm;
+                const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * Wa;
+                v += (di < 0.0) ? -kin : kin;
+                w.A[ki * p_init + kj] = v;
+            }
+        }
+
+        // ---- consistency iterations (:311-448)
+        for (int k = 0; k < p_init; ++k) {
+            w.x_old[k] = 0.0;
+            w.cur[k] = 1;
+        }
+        int count1 = 0;
+        while (true) {
+            double bmax = 0.0;
+            for (int k = 0; k < p_init; ++k)
+                if (w.cur[k]) bmax = fmax(bmax, fabs(w.b[k]));
+            if (!(bmax > tol1)) break;
+            count1 += 1;
+            if (count1 > o.max_solver) break;
+            // inactive_slip_removal (inactiveSlipRemoval.cc:4-124)
+            for (;;) {
+                int m = 0;
+                for (int k = 0; k < p_init; ++k)
+                    if (w.cur[k]) w.pos[m++] = (unsigned char)k;
+                for (int r = 0; r < m; ++r) {
+                    const int kr = w.pos[r];
+                    w.rhs[r] = w.b[kr];
+                    for (int c = 0; c < m; ++c) w.Apa[r * m + c] = w.A[kr * p_init + w.pos[c]];
+                }
+                double cnd = 1.0;
+                if (lu_solve(w.Apa, m, m, w.rhs, 1, 1, &cnd)) status |= QP_SINGULAR;
+                maxcond = fmax(maxcond, cnd);
+                ++rounds_total;
+                for (int k = 0; k < p_init; ++k) w.x[k] = 0.0;
+                for (int r = 0; r < m; ++r) w.x[w.pos[r]] = w.rhs[r];
+                bool removed = false;
+                for (int k = 0; k < p_init; ++k)
+                    if (w.cur[k] && (w.x_old[k] + w.x[k]) < 0) {
+                        w.cur[k] = 0;
+                        removed = true;
+                    }
+                if (!removed) break;
+            }
+            for (int k = 0; k < p_init; ++k) w.x_old[k] += w.x[k];
+            nPA = 0;
+            for (int k = 0; k < p_init; ++k) nPA += w.cur[k];
+
+            // del_FP (:337-357)
+            del_FP = zero3();
+            for (int k = 0; k < p_init; ++k) {
+                if (w.x_old[k] == 0.0) continue;
+                const int a = w.pa0[k];
+                const double sgn =
+                    ((w.tau_tr[k] - W_cur[(int64_t)a * cnt + i]) > 0) ? w.x_old[k] : -w.x_old[k];
+                M3 Sa;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) Sa.a[c] = w.Spa[k * 9 + c];
+                axpy(del_FP, sgn, Sa);
+            }
+            FP_tau = mul(matexp(del_FP, &e_terms, &status), FP_t2);
+            FE_tau = mul(F, inv(FP_tau));
+            Ce_tau = mulTN(FE_tau, FE_tau);
+            M3 E2 = Ce_tau;
+            E2(0, 0) -= 1.0;
+            E2(1, 1) -= 1.0;
+            E2(2, 2) -= 1.0;
+            E2 = scale(0.5, E2);
+            Tst = voigt_apply(D2, E2);
+            const M3 Xnc = mulTN(R, mul(mul(Ce_tau, Tst), R));
+            for (int k = 0; k < p_init; ++k) {
+                if (!w.cur[k]) continue;
+                const int a = w.pa0[k];
+                const double Wa = W_cur[(int64_t)a * cnt + i];
+                double t = resolved(L, a, Xnc);
+                if (a > ns - 1 && (w.tau_tr[k] - Wa) < 0) t = Wa;
+                w.tn[k] = t;
+            }
+            // hardening of every system (:399-429)
+            for (int a = 0; a < n; ++a) {
+                double h1 = 0.0;
+                for (int k = 0; k < p_init; ++k)
+                    if (w.x[k] != 0.0) h1 += ldg(&L.q[a * NM + w.pa0[k]]) * w.h[k] * w.x[k];
+                double sv = s_cur[(int64_t)a * cnt + i] + h1;
+                const double sat = ldg(&L.ss[a]);
+                if (sv > sat) sv = sat;
+                s_cur[(int64_t)a * cnt + i] = sv;
+            }
+            // backstress (:431-436) and b (:438-446) of the PA systems
+            for (int k = 0; k < p_init; ++k) {
+                const int a = w.pa0[k];
+                double& Wa = W_cur[(int64_t)a * cnt + i];
+                if ((w.tau_tr[k] - Wa) > 0)
+                    Wa = Wa + (ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa) * w.x[k];
+                else
+                    Wa = Wa + (-ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa) * w.x[k];
+            }
+            for (int k = 0; k < p_init; ++k)
+                if (w.cur[k]) {
+                    const int a = w.pa0[k];
+                    w.b[k] = fabs(w.tn[k] - W_cur[(int64_t)a * cnt + i]) - s_cur[(int64_t)a * cnt + i];
+                }
+        }
+
+        // ---- fractions (:450-456)
+        for (int t = 0; t < nw; ++t) {
+            double xo = 0.0;
+            for (int k = 0; k < p_init; ++k)
+                if (w.pa0[k] == ns + t) xo = w.x_old[k];
+            g.tw_i[(int64_t)t * cnt + i] = g.tw_c[(int64_t)t * cnt + i] + xo / L.twin_shear;
+        }
+        for (int t = 0; t < ns; ++t) {
+            double xo = 0.0;
+            for (int k = 0; k < p_init; ++k)
+                if (w.pa0[k] == t) xo = w.x_old[k];
+            g.sl_i[(int64_t)t * cnt + i] = g.sl_c[(int64_t)t * cnt + i] + xo;
+        }
+
+        // ---- stresses at the updated state (:458-468)
+        Fpn_inv = inv(FP_tau);
+        FE_tau = mul(F, Fpn_inv);
+        {
+            const double dFe = det(FE_tau);
+            const M3 t = scale(1.0 / dFe, mul(FE_tau, Tst));
+            T_tau = mulNT(t, FE_tau);
+            P_tau = scale(det(F), mulNT(T_tau, inv(F)));
+        }
+
+        if (flag == 1) {
+            // ---- tangent inside the slip-search loop (:473-828)
+            int p = 0;
+            for (int k = 0; k < p_init; ++k)
+                if (w.cur[k]) w.pos[p++] = (unsigned char)k;
+            for (int kl = 0; kl < 9; ++kl) {
+                const int kk = kl / 3, l = kl % 3;
+                M3 dFe;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) dFe(a, j) = (a == kk) ? Fpn_inv(l, j) : 0.0;
+                if (dFp_nonzero) {
+                    M3 X1;
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
+                    const M3 t = mul(mul(FE_tau, X1), Fpn_inv);
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) dFe.a[c] -= t.a[c];
+                }
+                const M3 G = mulTN(dFe, FE_tau);
+                M3 dE;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) dE(a, b) = 0.5 * (G(a, b) + G(b, a));
+                const M3 dT = voigt_apply(D2, dE);
+                M3 dtau = mul(Ce_tau, dT);
+                axpy(dtau, 2.0, mul(dE, Tst));
+                for (int r = 0; r < p; ++r) {
+                    const int k = w.pos[r];
+                    M3 Sk;
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) Sk.a[c] = w.Spa[k * 9 + c];
+                    double v = dot9(Sk, dtau);
+                    if (neg_t_bits >> w.pa0[k] & 1ull) v = -v;
+                    w.rhs[r * 9 + kl] = v;
+                }
+            }
+            {
+                double tol2 = 1.0;
+                int count3 = 0;
+                M3 t2 = eye3();
+                const double lim = fmax(tol1 / 1e4, 1e-12);
+                while (tol2 > lim) {
+                    if (count3 >= GATEAUX_TERM_CAP) {
+                        status |= QP_SERIES_CAP;
+                        break;
+                    }
+                    count3 += 1;
+                    M3 t1 = scale(1.0 / count3, mul(del_FP, t2));
+                    tol2 = frob(t1);
+                    t2 = t1;
+                }
+                c_terms = count3;
+            }
+            const M3 X6 = mul(CE_tr, matexp(scale(-1.0, del_FP), nullptr, &status));
+            // S_PA (9 x p, :734-796) lives in the consistency matrix's storage,
+            // which this pass no longer reads (PMAX^2 >= 9 PMAX >= 9 p)
+            double* SPA = w.A;
+            for (int cj = 0; cj < p; ++cj) {
+                const int kj = w.pos[cj];
+                const int bsys = w.pa0[kj];
+                M3 Sj;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) Sj.a[c] = w.Spa[kj * 9 + c];
+                M3 dm, dp;
+                gateaux_pair(Sj, del_FP, c_terms, dm, dp);
+                const M3 Y = sym(mulTN(dm, X6));
+                M3 Mj = mul(Ce_tau, voigt_apply(D2, Y));
+                axpy(Mj, 2.0, mul(Y, Tst));
+                const bool nj = (neg_t_bits >> bsys) & 1ull;
+                for (int ci = 0; ci < p; ++ci) {
+                    const int ki = w.pos[ci];
+                    const int asys = w.pa0[ki];
+                    M3 Si;
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) Si.a[c] = w.Spa[ki * 9 + c];
+                    const bool ni = (neg_t_bits >> asys) & 1ull;
+                    const double sm = dot9(Si, Mj);
+                    double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
+                    v += (ni ^ nj) ? -sm : sm;
+                    const double Wa = W_cur[(int64_t)asys * cnt + i];
+                    const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * Wa;
+                    v += ni ? -kin : kin;
+                    w.Apa[ci * p + cj] = v;
+                }
+                const M3 spa = mul(dp, FP_t2);
+#pragma unroll
+                for (int c = 0; c < 9; ++c) SPA[c * p + cj] = nj ? -spa.a[c] : spa.a[c];
+            }
+            if (lu_solve(w.Apa, p, p, w.rhs, 9, 9)) status |= QP_SINGULAR;
+            double nd[81];
+            if (dFp_nonzero) {
+                const M3 ex = matexp(del_FP, nullptr, &status);
+                for (int a = 0; a < 3; ++a)
+                    for (int j = 0; j < 3; ++j)
+                        for (int kl = 0; kl < 9; ++kl)
+                            nd[(3 * a + j) * 9 + kl] = ex(a, 0) * dFp[(0 + j) * 9 + kl] +
+                                                       ex(a, 1) * dFp[(3 + j) * 9 + kl] +
+                                                       ex(a, 2) * dFp[(6 + j) * 9 + kl];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 81; ++c) nd[c] = 0.0;
+            }
+            for (int r = 0; r < 9; ++r)
+                for (int kl = 0; kl < 9; ++kl) {
+                    double sacc = 0.0;
+                    for (int c = 0; c < p; ++c) sacc += SPA[r * p + c] * w.rhs[c * 9 + kl];
+                    nd[r * 9 + kl] += sacc;
+                }
+#pragma unroll
+            for (int c = 0; c < 81; ++c) dFp[c] = nd[c];
+            dFp_nonzero = true;
+        }
+        ++iter1;
+    }
+
+    // ---- final tangent (:835-940)
+    if (flag == 1 && out.dPdF) {
+        const M3 Finv = inv(F);
+        const M3 t1 = mulNT(Tst, mul(Finv, FE_tau));
+        const M3 t2 = mul(Finv, FE_tau);
+        const M3 t3 = mul(FE_tau, Tst);
+        const M3 Z = mulNT(mulNT(t3, F), Finv);
+        for (int kl = 0; kl < 9; ++kl) {
+            const int kk = kl / 3, l = kl % 3;
+            M3 dFe;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) dFe(a, j) = (a == kk) ? Fpn_inv(l, j) : 0.0;
+            if (dFp_nonzero) {
+                M3 X1;
+#pragma unroll
+                for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
+                const M3 t = mul(mul(FE_tau, X1), Fpn_inv);
+#pragma unroll
+                for (int c = 0; c < 9; ++c) dFe.a[c] -= t.a[c];
+            }
+            const M3 Y = mulTN(dFe, FE_tau);
+            M3 Ys;
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) Ys(a, b) = 0.5 * (Y(a, b) + Y(b, a));
+            const M3 dTs = voigt_apply(D2, Ys);
+            M3 PK = mul(dFe, t1);
+            axpy(PK, 1.0, mulNT(mul(FE_tau, dTs), t2));
+            axpy(PK, -1.0, mulNT(mul(t3, dFe), Finv));
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) PK(a, j) -= Finv(j, kk) * Z(a, l);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) out.dPdF[c * 9 + kl] = out.scale * PK.a[c];
+        }
+    }
+
+    // ---- outputs and history (:942-959); CRSS/backstress are already in _iter
+    if (out.P)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) out.P[c] = out.scale * P_tau.a[c];
+    if (out.T)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) out.T[c] = T_tau.a[c];
+    store_soa3(g.Fe_i, cnt, i, FE_tau);
+    store_soa3(g.Fp_i, cnt, i, FP_tau);
+
+    // ---- twin reorientation (:962-1019)
+    if (L.twinning) {
+        double F_T;
+        if (!o.multiphase)
+            F_T = (F_r > 0) ? L.twin_thr + (L.twin_sat * F_e / F_r) : L.twin_thr;
+        else
+            F_T = L.twin_thr;
+        if (F_T > 1.0) F_T = 1.0;
+        int pos = 0;
+        double tmax = g.tw_i[i];
+        for (int t = 1; t < nw; ++t) {
+            const double v = g.tw_i[(int64_t)t * cnt + i];
+            if (v > tmax) {
+                tmax = v;
+                pos = t;
+            }
+        }
+        if (g.twin_c[i] != 1 && F_r > 0 && tmax > F_T) {
+            const double dot = r0 * r0 + r1 * r1 + r2 * r2;
+            const double c = cos(atan(sqrt(dot)));
+            const double q2[4] = {c, c * r0, c * r1, c * r2};
+            const double q1[4] = {0.0, ldg(&L.nn[3 * (ns + pos)]), ldg(&L.nn[3 * (ns + pos) + 1]),
+                                  ldg(&L.nn[3 * (ns + pos) + 2])};
+            double qp[4];
+            const double a = q2[0], b = q1[0];
+            const double d1 = q1[1] * q2[1] + q1[2] * q2[2] + q1[3] * q2[3];
+            qp[0] = (a * b) - d1;
+            qp[1] = a * q1[1] + b * q2[1] + q2[2] * q1[3] - q1[2] * q2[3];
+            qp[2] = a * q1[2] + b * q2[2] - q2[1] * q1[3] + q1[1] * q2[3];
+            qp[3] = a * q1[3] + b * q2[3] + q2[1] * q1[2] - q1[1] * q2[2];
+            if (qp[0] < 0)
+                for (int t = 0; t < 4; ++t) qp[t] = -qp[t];
+            if (fabs(qp[0]) < 1e-4) qp[0] = 1e-4;
+            const double iq = 1 / qp[0];
+            for (int t = 0; t < 3; ++t) {
+                const double rr = qp[t + 1] * iq;
+                g.rot_i[(int64_t)t * cnt + i] = rr;
+                g.rotnew_i[(int64_t)t * cnt + i] = rr;
+            }
+            g.twin_i[i] = 1;
+            for (int t = 0; t < nw; ++t) s_cur[(int64_t)(ns + t) * cnt + i] = 100000;
+        }
+    }
+
+    bool finite = true;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) finite = finite && isfinite(P_tau.a[c]);
+    if (!finite) status |= QP_NONFINITE;
+    if (maxcond > 1e12) status |= QP_ILL_CONDITIONED;
+    if (stats_out) {
+        stats_out[0] = p0 < 0 ? 0 : p0;
+        stats_out[1] = nPA;
+        stats_out[2] = rounds_total;
+        stats_out[3] = e_terms;
+        stats_out[4] = c_terms;
+        stats_out[5] = iter1;
+        stats_out[6] = lattice_id;
+        stats_out[7] = maxcond >= 1e99 ? 99 : (int)ceil(log10(maxcond));
+    }
+    return status;
+}
+
+}  // namespace cp

@@ -8,7 +8,7 @@
 
 #include "../../include/cp_gpu.h"
 #include "../../oracle/cp_oracle.h"
-#include "../../plasticity_b200/csrc/cp_qp.cuh"
+#include "../../plasticity_b200/csrc/cp_qp2.cuh"
 
 using namespace cp;
 
@@ -47,6 +47,8 @@ void to_aos(const double* s, int64_t n, int w, double* a) {
         for (int c = 0; c < w; ++c) a[i * w + c] = s[c * n + i];
 }
 
+int g_variant = 0;  // 0: qp_update2 (compact), 1: qp_update (plain)
+
 template <int NT, int PMAX>
 void run_all(const LatDev& L, const Opts& o, const GroupDev& g, const double* F, int flag, double F_e, double F_r,
              double* P, double* T, double* dPdF, int32_t* stats, int32_t* status) {
@@ -59,12 +61,16 @@ void run_all(const LatDev& L, const Opts& o, const GroupDev& g, const double* F,
         out.T = T ? T + 9 * i : nullptr;
         out.dPdF = (dPdF && flag == 1) ? dPdF + 81 * i : nullptr;
         out.scale = 1.0;
-        const int st = qp_update<NT, PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0);
+        const int st = g_variant == 0
+                           ? qp_update2<PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0)
+                           : qp_update<NT, PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0);
         if (status) status[i] = st;
     }
 }
 
 }  // namespace
+
+extern "C" void emu_set_variant(int v) { g_variant = v; }
 
 extern "C" int emu_update(const cp_material_t* mat, const cp_options_t* opt, const or_state* st, const double* F,
                           int32_t flag, double F_e, double F_r, double* P, double* T, double* dPdF, int32_t* stats,
@@ -106,7 +112,7 @@ extern "C" int emu_update(const cp_material_t* mat, const cp_options_t* opt, con
     else if (nT <= 32)
         run_all<32, 32>(L, o, g, F, flag, F_e, F_r, P, T, dPdF, stats, status);
     else
-        run_all<64, 48>(L, o, g, F, flag, F_e, F_r, P, T, dPdF, stats, status);
+        run_all<64, 64>(L, o, g, F, flag, F_e, F_r, P, T, dPdF, stats, status);
     for (int k = 8; k < 16; ++k) to_aos(fields[k].soa.data(), n, fields[k].w, fields[k].aos);
     for (int64_t i = 0; i < n; ++i) st->twin_iter[i] = twin_i[i];
     return 0;
