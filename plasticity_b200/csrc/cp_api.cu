@@ -459,7 +459,7 @@ void sort_group(cp_handle* h, const Group& g, FSrc fs) {
 template <int PMAX, class FSrc>
 void launch_update2(cp_handle* h, const Group& g, FSrc fs, int flag, double F_e, double F_r, double* P, double* T,
                     double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
-    update2_kernel<PMAX, FSrc><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(
+    update2_kernel<PMAX, FSrc><<<blocks_for(g.count, UPDATE2_BLOCK), UPDATE2_BLOCK, 0, h->stream>>>(
         h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats, kF, kT,
         g.lattice);
 }

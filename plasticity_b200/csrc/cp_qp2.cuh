@@ -22,11 +22,34 @@ template <int PMAX>
 struct QpScratch2 {
     unsigned char pa0[PMAX], cur[PMAX], pos[PMAX];
     double tau_tr[PMAX], b[PMAX], h[PMAX], x_old[PMAX], x[PMAX], tn[PMAX];
-    double Spa[PMAX * 9];
+    double Sv[PMAX * 6];      // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n
     double A[PMAX * PMAX];    // packed, leading dimension p_init
     double Apa[PMAX * PMAX];  // packed, leading dimension m (or p for A2)
     double rhs[PMAX * 9];
 };
+
+// S : X = (R m)^T X (R n) for a Schmid tensor stored as its two vectors
+__host__ __device__ __forceinline__ double schmid_dot(const double* v, const M3& X) {
+    const double y0 = X(0, 0) * v[3] + X(0, 1) * v[4] + X(0, 2) * v[5];
+    const double y1 = X(1, 0) * v[3] + X(1, 1) * v[4] + X(1, 2) * v[5];
+    const double y2 = X(2, 0) * v[3] + X(2, 1) * v[4] + X(2, 2) * v[5];
+    return v[0] * y0 + v[1] * y1 + v[2] * y2;
+}
+__host__ __device__ __forceinline__ M3 schmid_of(const double* v) {
+    M3 S;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) S(i, j) = v[i] * v[3 + j];
+    return S;
+}
+__host__ __device__ __forceinline__ void schmid_vectors(const LatDev& L, int s, const M3& R, double* v) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        v[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
+        v[3 + i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
+    }
+}
 
 // Trial state of one slip-search pass (:160-196) and the potentially active
 // set count; shared by classify_kernel and qp_update2.
@@ -96,6 +119,10 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
     M3 T_tau, P_tau;
     double dFp[81];
     bool dFp_nonzero = false;
+    // With one slip-search pass (the shipped setting) the final tangent reads
+    // dFp = S_PA delgamma column by column from S_PA (kept in w.A) and
+    // delgamma (kept in w.rhs) instead of materialising the 9x9 dFp.
+    int lazy_p = -1;
     int nPA = 0, p0 = -1, rounds_total = 0, e_terms = 0, c_terms = 0;
     double maxcond = 1.0;
     int iter1 = 1;
@@ -150,27 +177,20 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         for (int k = 0; k < p_init; ++k) {
             const int a = w.pa0[k];
             w.h[k] = ldg(&L.h0[a]) * pow((1 - s_cur[(int64_t)a * cnt + i] / ldg(&L.ss[a])), ldg(&L.a[a]));
-            const M3 S = schmid(L, a, R);
-#pragma unroll
-            for (int c = 0; c < 9; ++c) w.Spa[k * 9 + c] = S.a[c];
+            schmid_vectors(L, a, R, w.Sv + 6 * k);
         }
         for (int kj = 0; kj < p_init; ++kj) {
             const int bsys = w.pa0[kj];
-            M3 Sj;
-#pragma unroll
-            for (int c = 0; c < 9; ++c) Sj.a[c] = w.Spa[kj * 9 + c];
+            const M3 Sj = schmid_of(w.Sv + 6 * kj);
             const M3 Y = sym(mul(CE_tr, Sj));
             M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
             axpy(Mj, 2.0, mul(Y, Tst_tr));
             const double dj = w.tau_tr[kj] - W_cur[(int64_t)bsys * cnt + i];
             for (int ki = 0; ki < p_init; ++ki) {
                 const int asys = w.pa0[ki];
-                M3 Si;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) Si.a[c] = w.Spa[ki * 9 + c];
                 const double Wa = W_cur[(int64_t)asys * cnt + i];
                 const double di = w.tau_tr[ki] - Wa;
-                const double sm = dot9(Si, Mj);
+                const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
                 double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
                 v += (di * dj < 0.0) ? -sm : sm;
                 const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * Wa;
@@ -227,10 +247,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 const int a = w.pa0[k];
                 const double sgn =
                     ((w.tau_tr[k] - W_cur[(int64_t)a * cnt + i]) > 0) ? w.x_old[k] : -w.x_old[k];
-                M3 Sa;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) Sa.a[c] = w.Spa[k * 9 + c];
-                axpy(del_FP, sgn, Sa);
+                axpy(del_FP, sgn, schmid_of(w.Sv + 6 * k));
             }
             FP_tau = mul(matexp(del_FP, &e_terms, &status), FP_t2);
             FE_tau = mul(F, inv(FP_tau));
@@ -331,10 +348,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 axpy(dtau, 2.0, mul(dE, Tst));
                 for (int r = 0; r < p; ++r) {
                     const int k = w.pos[r];
-                    M3 Sk;
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) Sk.a[c] = w.Spa[k * 9 + c];
-                    double v = dot9(Sk, dtau);
+                    double v = schmid_dot(w.Sv + 6 * k, dtau);
                     if (neg_t_bits >> w.pa0[k] & 1ull) v = -v;
                     w.rhs[r * 9 + kl] = v;
                 }
@@ -363,9 +377,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             for (int cj = 0; cj < p; ++cj) {
                 const int kj = w.pos[cj];
                 const int bsys = w.pa0[kj];
-                M3 Sj;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) Sj.a[c] = w.Spa[kj * 9 + c];
+                const M3 Sj = schmid_of(w.Sv + 6 * kj);
                 M3 dm, dp;
                 gateaux_pair(Sj, del_FP, c_terms, dm, dp);
                 const M3 Y = sym(mulTN(dm, X6));
@@ -375,11 +387,8 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 for (int ci = 0; ci < p; ++ci) {
                     const int ki = w.pos[ci];
                     const int asys = w.pa0[ki];
-                    M3 Si;
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) Si.a[c] = w.Spa[ki * 9 + c];
                     const bool ni = (neg_t_bits >> asys) & 1ull;
-                    const double sm = dot9(Si, Mj);
+                    const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
                     double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
                     v += (ni ^ nj) ? -sm : sm;
                     const double Wa = W_cur[(int64_t)asys * cnt + i];
@@ -392,6 +401,11 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 for (int c = 0; c < 9; ++c) SPA[c * p + cj] = nj ? -spa.a[c] : spa.a[c];
             }
             if (lu_solve(w.Apa, p, p, w.rhs, 9, 9)) status |= QP_SINGULAR;
+            if (o.max_search == 1) {  // this is the last pass: keep S_PA and delgamma
+                lazy_p = p;
+                ++iter1;
+                continue;
+            }
             double nd[81];
             if (dFp_nonzero) {
                 const M3 ex = matexp(del_FP, nullptr, &status);
@@ -432,10 +446,19 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             for (int a = 0; a < 3; ++a)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) dFe(a, j) = (a == kk) ? Fpn_inv(l, j) : 0.0;
-            if (dFp_nonzero) {
+            if (dFp_nonzero || lazy_p > 0) {
                 M3 X1;
+                if (lazy_p > 0) {
 #pragma unroll
-                for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
+                    for (int c = 0; c < 9; ++c) {
+                        double acc = 0.0;
+                        for (int r = 0; r < lazy_p; ++r) acc += w.A[c * lazy_p + r] * w.rhs[r * 9 + kl];
+                        X1.a[c] = acc;
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
+                }
                 const M3 t = mul(mul(FE_tau, X1), Fpn_inv);
 #pragma unroll
                 for (int c = 0; c < 9; ++c) dFe.a[c] -= t.a[c];
