@@ -223,10 +223,11 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
 // calculatePlasticity over one group in sorted order (thread j runs internal
 // qp perm[j]).  Outputs by caller index k: P/T/dPdF/status/stats; with a
 // non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
-// update2 runs one warp per block; warps take the sorted (descending
-// active-set size) qps alternately from the front and the back, so every SM
-// holds a mix of large- and small-solve warps.
-constexpr int UPDATE2_BLOCK = 32;
+// Threads run the qps in sorted order (descending potentially-active-set
+// size): consecutive threads, and so the lanes of a warp, run solves of
+// similar size.  (Interleaving large- and small-solve warps across SMs and
+// sorting only inside 256-qp blocks both measured slower.)
+constexpr int UPDATE2_BLOCK = 256;
 
 template <int PMAX, class FSrc>
 __global__ void __launch_bounds__(UPDATE2_BLOCK) update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs,
@@ -236,10 +237,7 @@ __global__ void __launch_bounds__(UPDATE2_BLOCK) update2_kernel(const LatDev* __
                                                            int32_t* __restrict__ status, int32_t* __restrict__ stats,
                                                            double* __restrict__ keepF, double* __restrict__ keepT,
                                                            int lattice_id) {
-    const int64_t W = (g.count + 31) / 32;
-    const int64_t w = blockIdx.x;
-    const int64_t ws = (w & 1) ? (W - 1 - (w >> 1)) : (w >> 1);
-    const int64_t j = ws * 32 + threadIdx.x;
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= g.count) return;
     const int64_t i = perm[j];
     const int64_t k = g.qp[i];
