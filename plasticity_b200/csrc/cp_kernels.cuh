@@ -225,21 +225,24 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
 // non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
 // Threads run the qps in sorted order (descending potentially-active-set
 // size): consecutive threads, and so the lanes of a warp, run solves of
-// similar size.  (Interleaving large- and small-solve warps across SMs and
-// sorting only inside 256-qp blocks both measured slower.)
+// similar size.  (Interleaving large- and small-solve warps across SMs,
+// sorting only inside 256-qp blocks, and a persistent grid-stride launch with
+// 64-256 resident threads per SM all measured slower.)
 constexpr int UPDATE2_BLOCK = 256;
+// Resident blocks per SM the compiler sizes registers for: 1 (up to 255
+// registers) for the small FCC-class solve, 2 (128 registers, twice the warps
+// to hide local-memory latency, more spills) for the BCC/HCP classes, whose
+// longer solves gain more from the extra warps than they lose to the spills
+// (measured per class).
+constexpr int update2_min_blocks(int pmax) { return pmax <= 16 ? 1 : 2; }
 
 template <int PMAX, class FSrc>
-__global__ void __launch_bounds__(UPDATE2_BLOCK) update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs,
-                                                           const int* __restrict__ perm, int flag, double F_e,
-                                                           double F_r, double* __restrict__ P, double* __restrict__ T,
-                                                           double* __restrict__ dPdF, double* __restrict__ stage,
-                                                           int32_t* __restrict__ status, int32_t* __restrict__ stats,
-                                                           double* __restrict__ keepF, double* __restrict__ keepT,
-                                                           int lattice_id) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= g.count) return;
-    const int64_t i = perm[j];
+__device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, const GroupDev& g, const FSrc& fs,
+                                            int64_t i, int flag, double F_e, double F_r, double* __restrict__ P,
+                                            double* __restrict__ T, double* __restrict__ dPdF,
+                                            double* __restrict__ stage, int32_t* __restrict__ status,
+                                            int32_t* __restrict__ stats, double* __restrict__ keepF,
+                                            double* __restrict__ keepT, int lattice_id) {
     const int64_t k = g.qp[i];
     const M3 F = fs(k);
     double Tl[9];
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(UPDATE2_BLOCK) update2_kernel(const LatDev* __
         out.scale = 1.0;
     }
     out.T = (T || keepT) ? Tl : nullptr;
-    const int st = qp_update2<PMAX>(*L, o, g, i, F, flag, F_e, F_r, out, stats ? stats + 8 * k : nullptr, lattice_id);
+    const int st = qp_update2<PMAX>(L, o, g, i, F, flag, F_e, F_r, out, stats ? stats + 8 * k : nullptr, lattice_id);
     if (T)
 #pragma unroll
         for (int c = 0; c < 9; ++c) T[9 * k + c] = Tl[c];
@@ -266,6 +269,18 @@ __global__ void __launch_bounds__(UPDATE2_BLOCK) update2_kernel(const LatDev* __
         }
     }
     if (status) status[k] = st;
+}
+
+template <int PMAX, class FSrc>
+__global__ void __launch_bounds__(UPDATE2_BLOCK, update2_min_blocks(PMAX))
+    update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs, const int* __restrict__ perm, int flag,
+                   double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
+                   double* __restrict__ stage, int32_t* __restrict__ status, int32_t* __restrict__ stats,
+                   double* __restrict__ keepF, double* __restrict__ keepT, int lattice_id) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < g.count)
+        update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
+                          lattice_id);
 }
 
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P

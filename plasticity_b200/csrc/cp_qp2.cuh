@@ -8,8 +8,12 @@
 //     warp), and the _iter arrays of CRSS and backstress are the working
 //     storage of the current values (initialised from _conv on entry);
 //   * per-thread arrays are compact over the potentially active set of the
-//     current pass (capacity PMAX), and the consistency matrix is packed at its
-//     actual size, so the touched scratch grows with p0^2, not PMAX^2;
+//     current pass (capacity PMAX), so the touched scratch grows with p0^2, not
+//     PMAX^2.  The matrices that are solved (removal rounds, tangent) use the
+//     row stride PMAX, not their size: local memory is interleaved across the
+//     lanes of a warp and coalesces only when every lane addresses the same
+//     relative offset, which a fixed stride keeps true while the lanes' active
+//     sets shrink to different sizes;
 //   * qps arrive sorted by potentially-active-set size (classify_kernel +
 //     counting sort), so the threads of a warp run solves of similar size.
 #pragma once
@@ -21,10 +25,10 @@ namespace cp {
 template <int PMAX>
 struct QpScratch2 {
     unsigned char pa0[PMAX], cur[PMAX], pos[PMAX];
-    double tau_tr[PMAX], b[PMAX], h[PMAX], x_old[PMAX], x[PMAX], tn[PMAX];
+    double tau_tr[PMAX], b[PMAX], h[PMAX], x_old[PMAX], x[PMAX], tn[PMAX], kin[PMAX];
     double Sv[PMAX * 6];      // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n
     double A[PMAX * PMAX];    // packed, leading dimension p_init
-    double Apa[PMAX * PMAX];  // packed, leading dimension m (or p for A2)
+    double Apa[PMAX * PMAX];  // leading dimension PMAX
     double rhs[PMAX * 9];
 };
 
@@ -49,6 +53,94 @@ __host__ __device__ __forceinline__ void schmid_vectors(const LatDev& L, int s, 
         v[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
         v[3 + i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
     }
+}
+
+// a_i[c] -= f a_j[c] for c in [c0, m) on two distinct rows of one matrix.
+// Four columns per step, all loads before the stores: with rows of one array
+// the compiler must otherwise assume a store may feed the next load and runs
+// the loop one memory round trip per column.  Same operation per element.
+__host__ __device__ __forceinline__ void row_axpy(double* ai, const double* aj, double f, int c0, int m) {
+    int c = c0;
+    for (; c + 4 <= m; c += 4) {
+        const double x0 = aj[c], x1 = aj[c + 1], x2 = aj[c + 2], x3 = aj[c + 3];
+        const double y0 = ai[c], y1 = ai[c + 1], y2 = ai[c + 2], y3 = ai[c + 3];
+        ai[c] = y0 - f * x0;
+        ai[c + 1] = y1 - f * x1;
+        ai[c + 2] = y2 - f * x2;
+        ai[c + 3] = y3 - f * x3;
+    }
+    for (; c < m; ++c) ai[c] -= f * aj[c];
+}
+__host__ __device__ __forceinline__ void row_swap(double* a, double* b, int m) {
+    int c = 0;
+    for (; c + 4 <= m; c += 4) {
+        const double x0 = a[c], x1 = a[c + 1], x2 = a[c + 2], x3 = a[c + 3];
+        const double y0 = b[c], y1 = b[c + 1], y2 = b[c + 2], y3 = b[c + 3];
+        a[c] = y0, a[c + 1] = y1, a[c + 2] = y2, a[c + 3] = y3;
+        b[c] = x0, b[c + 1] = x1, b[c + 2] = x2, b[c + 3] = x3;
+    }
+    for (; c < m; ++c) {
+        const double t = a[c];
+        a[c] = b[c];
+        b[c] = t;
+    }
+}
+
+// lu_solve (cp_qp.cuh) with the batched row operations above and NRHS known
+// at compile time: Gaussian elimination with partial pivoting on the rows,
+// same pivots and same arithmetic per element, so the same results.
+template <int NRHS>
+__host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, double* B, double* cond = nullptr) {
+    int sing = 0;
+    double pmin = 1e308, pmax = 0.0;
+    for (int j = 0; j < m; ++j) {
+        int r = j;
+        double mx = fabs(A[j * ld + j]);
+        for (int i = j + 1; i < m; ++i) {
+            const double v = fabs(A[i * ld + j]);
+            if (v > mx) {
+                mx = v;
+                r = i;
+            }
+        }
+        pmin = fmin(pmin, mx);
+        pmax = fmax(pmax, mx);
+        if (mx == 0.0) {
+            sing = 1;
+            continue;
+        }
+        if (r != j) {
+            row_swap(A + j * ld, A + r * ld, m);
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) {
+                const double t = B[j * NRHS + c];
+                B[j * NRHS + c] = B[r * NRHS + c];
+                B[r * NRHS + c] = t;
+            }
+        }
+        const double piv = 1.0 / A[j * ld + j];
+        double bj[NRHS];
+#pragma unroll
+        for (int c = 0; c < NRHS; ++c) bj[c] = B[j * NRHS + c];
+        for (int i = j + 1; i < m; ++i) {
+            const double f = A[i * ld + j] * piv;
+            if (f == 0.0) continue;
+            row_axpy(A + i * ld, A + j * ld, f, j + 1, m);
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) B[i * NRHS + c] -= f * bj[c];
+        }
+    }
+    for (int j = m - 1; j >= 0; --j) {
+        const double d = A[j * ld + j];
+#pragma unroll
+        for (int c = 0; c < NRHS; ++c) {
+            double s = B[j * NRHS + c];
+            for (int k = j + 1; k < m; ++k) s -= A[j * ld + k] * B[k * NRHS + c];
+            B[j * NRHS + c] = s / d;
+        }
+    }
+    if (cond) *cond = m == 0 ? 1.0 : (pmin > 0.0 ? pmax / pmin : 1e308);
+    return sing;
 }
 
 // Trial state of one slip-search pass (:160-196) and the potentially active
@@ -102,11 +194,14 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
     double* __restrict__ s_cur = g.s_i;  // current CRSS of every system, [a * cnt + i]
     double* __restrict__ W_cur = g.W_i;  // current backstress
 
-    // ---- history (:28-35): the _iter CRSS/backstress start as the _conv values
-    for (int a = 0; a < n; ++a) {
-        s_cur[(int64_t)a * cnt + i] = g.s_c[(int64_t)a * cnt + i];
-        W_cur[(int64_t)a * cnt + i] = g.W_c[(int64_t)a * cnt + i];
-    }
+    // ---- history (:28-35): the _iter CRSS/backstress start as the _conv
+    // values; the first pass's potentially-active-set loop copies them as it
+    // reads them (here only when there is no pass at all)
+    if (o.max_search < 1)
+        for (int a = 0; a < n; ++a) {
+            s_cur[(int64_t)a * cnt + i] = g.s_c[(int64_t)a * cnt + i];
+            W_cur[(int64_t)a * cnt + i] = g.W_c[(int64_t)a * cnt + i];
+        }
     const double r0 = g.rot_c[i], r1 = g.rot_c[cnt + i], r2 = g.rot_c[2 * cnt + i];
     const M3 R = odfpoint(r0, r1, r2);
     const Sym6 D2 = elasticmoduli(R, L.C);
@@ -148,10 +243,19 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         // ---- resolved shears, potentially active set (:199-244), compact
         nPA = 0;
         for (int a = 0; a < n; ++a) {
-            const double W = W_cur[(int64_t)a * cnt + i];
+            double W, sa;
+            if (iter1 == 1) {
+                W = g.W_c[(int64_t)a * cnt + i];
+                sa = g.s_c[(int64_t)a * cnt + i];
+                W_cur[(int64_t)a * cnt + i] = W;
+                s_cur[(int64_t)a * cnt + i] = sa;
+            } else {
+                W = W_cur[(int64_t)a * cnt + i];
+                sa = s_cur[(int64_t)a * cnt + i];
+            }
             double t = resolved(L, a, tr.Xc);
             if (a > ns - 1 && (t - W) < 0) t = W;
-            const double bb = fabs(t - W) - s_cur[(int64_t)a * cnt + i];
+            const double bb = fabs(t - W) - sa;
             if (bb >= tol1) {
                 if (nPA < PMAX) {
                     w.pa0[nPA] = (unsigned char)a;
@@ -174,10 +278,20 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         }
 
         // ---- h_beta (:252-262) and A[PA,PA] (:265-306), packed p_init x p_init
+        // Row constants first: bit k of neg_d is the sign of tau_tr - W of PA
+        // entry k, w.kin[k] the signed kinematic term of its row.  The
+        // reference's sign test di * dj < 0 equals neg_d_i != neg_d_j here,
+        // since |tau_tr - W| >= s + tol > 0 for every PA member.
+        unsigned long long neg_d = 0ull;
         for (int k = 0; k < p_init; ++k) {
             const int a = w.pa0[k];
             w.h[k] = ldg(&L.h0[a]) * pow((1 - s_cur[(int64_t)a * cnt + i] / ldg(&L.ss[a])), ldg(&L.a[a]));
             schmid_vectors(L, a, R, w.Sv + 6 * k);
+            const double Wa = W_cur[(int64_t)a * cnt + i];
+            const double kin = ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa;
+            const bool ng = (w.tau_tr[k] - Wa) < 0.0;
+            if (ng) neg_d |= (1ull << k);
+            w.kin[k] = ng ? -kin : kin;
         }
         for (int kj = 0; kj < p_init; ++kj) {
             const int bsys = w.pa0[kj];
@@ -185,16 +299,14 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             const M3 Y = sym(mul(CE_tr, Sj));
             M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
             axpy(Mj, 2.0, mul(Y, Tst_tr));
-            const double dj = w.tau_tr[kj] - W_cur[(int64_t)bsys * cnt + i];
+            const unsigned long long nj = (neg_d >> kj) & 1ull;
+            const double hj = w.h[kj];
             for (int ki = 0; ki < p_init; ++ki) {
                 const int asys = w.pa0[ki];
-                const double Wa = W_cur[(int64_t)asys * cnt + i];
-                const double di = w.tau_tr[ki] - Wa;
                 const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
-                double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
-                v += (di * dj < 0.0) ? -sm : sm;
-                const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * Wa;
-                v += (di < 0.0) ? -kin : kin;
+                double v = ldg(&L.q[asys * NM + bsys]) * hj;
+                v += (((neg_d >> ki) & 1ull) ^ nj) ? -sm : sm;
+                v += w.kin[ki];
                 w.A[ki * p_init + kj] = v;
             }
         }
@@ -220,10 +332,10 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 for (int r = 0; r < m; ++r) {
                     const int kr = w.pos[r];
                     w.rhs[r] = w.b[kr];
-                    for (int c = 0; c < m; ++c) w.Apa[r * m + c] = w.A[kr * p_init + w.pos[c]];
+                    for (int c = 0; c < m; ++c) w.Apa[r * PMAX + c] = w.A[kr * p_init + w.pos[c]];
                 }
                 double cnd = 1.0;
-                if (lu_solve(w.Apa, m, m, w.rhs, 1, 1, &cnd)) status |= QP_SINGULAR;
+                if (lu_solve_b<1>(w.Apa, m, PMAX, w.rhs, &cnd)) status |= QP_SINGULAR;
                 maxcond = fmax(maxcond, cnd);
                 ++rounds_total;
                 for (int k = 0; k < p_init; ++k) w.x[k] = 0.0;
@@ -267,11 +379,40 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 if (a > ns - 1 && (w.tau_tr[k] - Wa) < 0) t = Wa;
                 w.tn[k] = t;
             }
-            // hardening of every system (:399-429)
+            // hardening of every system (:399-429).  Only systems with a
+            // non-zero increment contribute; up to four of them (the usual
+            // case) are gathered into registers once, in PA order, so the sum
+            // over them is the same sequence of operations as the full loop.
+            int nzc = 0, za0 = 0, za1 = 0, za2 = 0, za3 = 0;
+            double zh0 = 0.0, zh1 = 0.0, zh2 = 0.0, zh3 = 0.0, zx0 = 0.0, zx1 = 0.0, zx2 = 0.0, zx3 = 0.0;
+            for (int k = 0; k < p_init; ++k) {
+                const double xk = w.x[k];
+                if (xk == 0.0) continue;
+                const int ak = w.pa0[k];
+                const double hk = w.h[k];
+                if (nzc == 0) {
+                    za0 = ak; zh0 = hk; zx0 = xk;
+                } else if (nzc == 1) {
+                    za1 = ak; zh1 = hk; zx1 = xk;
+                } else if (nzc == 2) {
+                    za2 = ak; zh2 = hk; zx2 = xk;
+                } else if (nzc == 3) {
+                    za3 = ak; zh3 = hk; zx3 = xk;
+                }
+                ++nzc;
+            }
             for (int a = 0; a < n; ++a) {
                 double h1 = 0.0;
-                for (int k = 0; k < p_init; ++k)
-                    if (w.x[k] != 0.0) h1 += ldg(&L.q[a * NM + w.pa0[k]]) * w.h[k] * w.x[k];
+                if (nzc <= 4) {
+                    const double* qa = L.q + a * NM;
+                    if (nzc > 0) h1 += ldg(&qa[za0]) * zh0 * zx0;
+                    if (nzc > 1) h1 += ldg(&qa[za1]) * zh1 * zx1;
+                    if (nzc > 2) h1 += ldg(&qa[za2]) * zh2 * zx2;
+                    if (nzc > 3) h1 += ldg(&qa[za3]) * zh3 * zx3;
+                } else {
+                    for (int k = 0; k < p_init; ++k)
+                        if (w.x[k] != 0.0) h1 += ldg(&L.q[a * NM + w.pa0[k]]) * w.h[k] * w.x[k];
+                }
                 double sv = s_cur[(int64_t)a * cnt + i] + h1;
                 const double sat = ldg(&L.ss[a]);
                 if (sv > sat) sv = sat;
@@ -294,17 +435,16 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         }
 
         // ---- fractions (:450-456)
-        for (int t = 0; t < nw; ++t) {
-            double xo = 0.0;
-            for (int k = 0; k < p_init; ++k)
-                if (w.pa0[k] == ns + t) xo = w.x_old[k];
-            g.tw_i[(int64_t)t * cnt + i] = g.tw_c[(int64_t)t * cnt + i] + xo / L.twin_shear;
-        }
-        for (int t = 0; t < ns; ++t) {
-            double xo = 0.0;
-            for (int k = 0; k < p_init; ++k)
-                if (w.pa0[k] == t) xo = w.x_old[k];
-            g.sl_i[(int64_t)t * cnt + i] = g.sl_c[(int64_t)t * cnt + i] + xo;
+        // Systems outside PA get _conv + 0, PA systems _conv + their total
+        // increment (PA members are distinct systems).
+        for (int t = 0; t < nw; ++t) g.tw_i[(int64_t)t * cnt + i] = g.tw_c[(int64_t)t * cnt + i] + 0.0;
+        for (int t = 0; t < ns; ++t) g.sl_i[(int64_t)t * cnt + i] = g.sl_c[(int64_t)t * cnt + i] + 0.0;
+        for (int k = 0; k < p_init; ++k) {
+            const int a = w.pa0[k];
+            if (a < ns)
+                g.sl_i[(int64_t)a * cnt + i] = g.sl_c[(int64_t)a * cnt + i] + w.x_old[k];
+            else
+                g.tw_i[(int64_t)(a - ns) * cnt + i] = g.tw_c[(int64_t)(a - ns) * cnt + i] + w.x_old[k] / L.twin_shear;
         }
 
         // ---- stresses at the updated state (:458-468)
@@ -394,13 +534,13 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                     const double Wa = W_cur[(int64_t)asys * cnt + i];
                     const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * Wa;
                     v += ni ? -kin : kin;
-                    w.Apa[ci * p + cj] = v;
+                    w.Apa[ci * PMAX + cj] = v;
                 }
                 const M3 spa = mul(dp, FP_t2);
 #pragma unroll
-                for (int c = 0; c < 9; ++c) SPA[c * p + cj] = nj ? -spa.a[c] : spa.a[c];
+                for (int c = 0; c < 9; ++c) SPA[c * PMAX + cj] = nj ? -spa.a[c] : spa.a[c];
             }
-            if (lu_solve(w.Apa, p, p, w.rhs, 9, 9)) status |= QP_SINGULAR;
+            if (lu_solve_b<9>(w.Apa, p, PMAX, w.rhs)) status |= QP_SINGULAR;
             if (o.max_search == 1) {  // this is the last pass: keep S_PA and delgamma
                 lazy_p = p;
                 ++iter1;
@@ -422,7 +562,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             for (int r = 0; r < 9; ++r)
                 for (int kl = 0; kl < 9; ++kl) {
                     double sacc = 0.0;
-                    for (int c = 0; c < p; ++c) sacc += SPA[r * p + c] * w.rhs[c * 9 + kl];
+                    for (int c = 0; c < p; ++c) sacc += SPA[r * PMAX + c] * w.rhs[c * 9 + kl];
                     nd[r * 9 + kl] += sacc;
                 }
 #pragma unroll
@@ -452,7 +592,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
 #pragma unroll
                     for (int c = 0; c < 9; ++c) {
                         double acc = 0.0;
-                        for (int r = 0; r < lazy_p; ++r) acc += w.A[c * lazy_p + r] * w.rhs[r * 9 + kl];
+                        for (int r = 0; r < lazy_p; ++r) acc += w.A[c * PMAX + r] * w.rhs[r * 9 + kl];
                         X1.a[c] = acc;
                     }
                 } else {
