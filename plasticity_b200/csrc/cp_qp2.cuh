@@ -22,14 +22,18 @@
 
 namespace cp {
 
-template <int PMAX>
-struct QpScratch2 {
-    unsigned char pa0[PMAX], cur[PMAX], pos[PMAX];
-    double tau_tr[PMAX], b[PMAX], h[PMAX], x_old[PMAX], x[PMAX], tn[PMAX], kin[PMAX];
-    double Sv[PMAX * 6];      // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n
-    double A[PMAX * PMAX];    // packed, leading dimension p_init
-    double Apa[PMAX * PMAX];  // leading dimension PMAX
-    double rhs[PMAX * 9];
+// Per-thread scratch of qp_update2: each array is its own local variable and
+// this struct only points at them.  Arrays that are fields of one local
+// struct, indexed at run time, may alias as far as the compiler can tell, so
+// every scratch store would order the loads after it; distinct variables
+// cannot alias, which leaves it free to batch loads.
+struct Scratch2 {
+    unsigned char *pa0, *cur, *pos;
+    double *tau_tr, *b, *h, *x_old, *x, *tn, *kin;
+    double* Sv;   // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n (6 per k)
+    double* A;    // consistency matrix, leading dimension p_init
+    double* Apa;  // the matrix being solved, leading dimension PMAX
+    double* rhs;  // right-hand sides, 9 per row
 };
 
 // S : X = (R m)^T X (R n) for a Schmid tensor stored as its two vectors
@@ -186,7 +190,10 @@ __host__ __device__ __forceinline__ int count_potentially_active(const LatDev& L
 template <int PMAX>
 __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
                                    double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id) {
-    QpScratch2<PMAX> w;
+    unsigned char pa0_[PMAX], cur_[PMAX], pos_[PMAX];
+    double tau_tr_[PMAX], b_[PMAX], h_[PMAX], x_old_[PMAX], x_[PMAX], tn_[PMAX], kin_[PMAX];
+    double Sv_[PMAX * 6], A_[PMAX * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
+    const Scratch2 w{pa0_, cur_, pos_, tau_tr_, b_, h_, x_old_, x_, tn_, kin_, Sv_, A_, Apa_, rhs_};
     const int n = L.n, ns = L.ns, nw = L.nw;
     const int64_t cnt = g.count;
     int status = 0;
