@@ -242,7 +242,8 @@ __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, cons
                                             double* __restrict__ T, double* __restrict__ dPdF,
                                             double* __restrict__ stage, int32_t* __restrict__ status,
                                             int32_t* __restrict__ stats, double* __restrict__ keepF,
-                                            double* __restrict__ keepT, int lattice_id) {
+                                            double* __restrict__ keepT, int lattice_id, double* d2_slot,
+                                            int d2_stride) {
     const int64_t k = g.qp[i];
     const M3 F = fs(k);
     double Tl[9];
@@ -257,7 +258,8 @@ __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, cons
         out.scale = 1.0;
     }
     out.T = (T || keepT) ? Tl : nullptr;
-    const int st = qp_update2<PMAX>(L, o, g, i, F, flag, F_e, F_r, out, stats ? stats + 8 * k : nullptr, lattice_id);
+    const int st = qp_update2<PMAX>(L, o, g, i, F, flag, F_e, F_r, out, stats ? stats + 8 * k : nullptr, lattice_id,
+                                    d2_slot, d2_stride);
     if (T)
 #pragma unroll
         for (int c = 0; c < 9; ++c) T[9 * k + c] = Tl[c];
@@ -277,10 +279,12 @@ __global__ void __launch_bounds__(UPDATE2_BLOCK, update2_min_blocks(PMAX))
                    double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
                    double* __restrict__ stage, int32_t* __restrict__ status, int32_t* __restrict__ stats,
                    double* __restrict__ keepF, double* __restrict__ keepT, int lattice_id) {
+    // per-thread rotated-stiffness slots, entry e of thread t at sD2[e * UPDATE2_BLOCK + t]
+    __shared__ double sD2[21 * UPDATE2_BLOCK];
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < g.count)
         update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
-                          lattice_id);
+                          lattice_id, sD2 + threadIdx.x, UPDATE2_BLOCK);
 }
 
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P

@@ -139,10 +139,26 @@ struct Sym6 {
     }
 };
 
+// The same 21 entries held elsewhere (e.g. a per-thread slot in shared
+// memory, entry e at p[e * stride]).
+struct Sym6Ref {
+    const double* p;
+    int stride;
+    CP_HD double operator()(int i, int j) const {
+        if (i > j) {
+            const int t = i;
+            i = j;
+            j = t;
+        }
+        return p[(i * 6 - i * (i - 1) / 2 + (j - i)) * stride];
+    }
+};
+
 // matform(D * vecform_eng(X)): stress from a symmetric strain-like tensor,
 // with the engineering-shear doubling of the reference's Dmat
 // (calculatePlasticity.cc:64-68) applied to the shear inputs.
-CP_HD M3 voigt_apply(const Sym6& D, const M3& X) {
+template <class SymD>
+CP_HD M3 voigt_apply(const SymD& D, const M3& X) {
     const double v0 = X(0, 0), v1 = X(1, 1), v2 = X(2, 2);
     const double v3 = 2.0 * X(1, 2), v4 = 2.0 * X(0, 2), v5 = 2.0 * X(0, 1);
     double w[6];

@@ -147,13 +147,58 @@ __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, dou
     return sing;
 }
 
+// Final tangent (:835-940) from the converged kinematics: for each kl,
+// dFe = d(Fe)/dF_kl = E_kl Fp^-1 - Fe dFp_kl Fp^-1 (x1(kl, X) gives the
+// column dFp_kl and returns false when dFp is zero), the stress derivative and
+// the reference's PK_Stiff5 terms as written; dPdF[c * 9 + kl] = scale * PK.
+template <class SymD, class X1Src>
+__host__ __device__ __forceinline__ void final_tangent(const M3& F, const M3& FE_tau, const M3& Fpn_inv, const M3& Tst,
+                                                       const SymD& D2, const X1Src& x1, double scale, double* dPdF) {
+    const M3 Finv = inv(F);
+    const M3 t1 = mulNT(Tst, mul(Finv, FE_tau));
+    const M3 t2 = mul(Finv, FE_tau);
+    const M3 t3 = mul(FE_tau, Tst);
+    const M3 Z = mulNT(mulNT(t3, F), Finv);
+    for (int kl = 0; kl < 9; ++kl) {
+        const int kk = kl / 3, l = kl % 3;
+        M3 dFe;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) dFe(a, j) = (a == kk) ? Fpn_inv(l, j) : 0.0;
+        M3 X1;
+        if (x1(kl, X1)) {
+            const M3 t = mul(mul(FE_tau, X1), Fpn_inv);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) dFe.a[c] -= t.a[c];
+        }
+        const M3 Y = mulTN(dFe, FE_tau);
+        M3 Ys;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) Ys(a, b) = 0.5 * (Y(a, b) + Y(b, a));
+        const M3 dTs = voigt_apply(D2, Ys);
+        M3 PK = mul(dFe, t1);
+        axpy(PK, 1.0, mulNT(mul(FE_tau, dTs), t2));
+        axpy(PK, -1.0, mulNT(mul(t3, dFe), Finv));
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) PK(a, j) -= Finv(j, kk) * Z(a, l);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) dPdF[c * 9 + kl] = scale * PK.a[c];
+    }
+}
+
 // Trial state of one slip-search pass (:160-196) and the potentially active
 // set count; shared by classify_kernel and qp_update2.
 struct Trial {
     M3 Fpn_inv, CE, Tst, Xc;
 };
 
-__host__ __device__ __forceinline__ Trial trial_state(const M3& F, const M3& FP, const Sym6& D2, const M3& R) {
+template <class SymD>
+__host__ __device__ __forceinline__ Trial trial_state(const M3& F, const M3& FP, const SymD& D2, const M3& R) {
     Trial t;
     t.Fpn_inv = inv(FP);
     const M3 FE = mul(F, t.Fpn_inv);
@@ -189,7 +234,8 @@ __host__ __device__ __forceinline__ int count_potentially_active(const LatDev& L
 
 template <int PMAX>
 __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
-                                   double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id) {
+                                   double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id,
+                                   double* d2_slot, int d2_stride) {
     unsigned char pa0_[PMAX], cur_[PMAX], pos_[PMAX];
     double tau_tr_[PMAX], b_[PMAX], h_[PMAX], x_old_[PMAX], x_[PMAX], tn_[PMAX], kin_[PMAX];
     double Sv_[PMAX * 6], A_[PMAX * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
@@ -211,7 +257,14 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         }
     const double r0 = g.rot_c[i], r1 = g.rot_c[cnt + i], r2 = g.rot_c[2 * cnt + i];
     const M3 R = odfpoint(r0, r1, r2);
-    const Sym6 D2 = elasticmoduli(R, L.C);
+    // the rotated stiffness lives in the caller's slot (shared memory in the
+    // kernel: 21 doubles that would otherwise hold registers all along)
+    {
+        const Sym6 D2v = elasticmoduli(R, L.C);
+#pragma unroll
+        for (int e = 0; e < 21; ++e) d2_slot[e * d2_stride] = D2v.c[e];
+    }
+    const Sym6Ref D2{d2_slot, d2_stride};
 
     unsigned long long neg_t_bits = 0ull;
     M3 FP_tau = load_soa3(g.Fp_c, cnt, i);
@@ -579,57 +632,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         ++iter1;
     }
 
-    // ---- final tangent (:835-940)
-    if (flag == 1 && out.dPdF) {
-        const M3 Finv = inv(F);
-        const M3 t1 = mulNT(Tst, mul(Finv, FE_tau));
-        const M3 t2 = mul(Finv, FE_tau);
-        const M3 t3 = mul(FE_tau, Tst);
-        const M3 Z = mulNT(mulNT(t3, F), Finv);
-        for (int kl = 0; kl < 9; ++kl) {
-            const int kk = kl / 3, l = kl % 3;
-            M3 dFe;
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) dFe(a, j) = (a == kk) ? Fpn_inv(l, j) : 0.0;
-            if (dFp_nonzero || lazy_p > 0) {
-                M3 X1;
-                if (lazy_p > 0) {
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) {
-                        double acc = 0.0;
-                        for (int r = 0; r < lazy_p; ++r) acc += w.A[c * PMAX + r] * w.rhs[r * 9 + kl];
-                        X1.a[c] = acc;
-                    }
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
-                }
-                const M3 t = mul(mul(FE_tau, X1), Fpn_inv);
-#pragma unroll
-                for (int c = 0; c < 9; ++c) dFe.a[c] -= t.a[c];
-            }
-            const M3 Y = mulTN(dFe, FE_tau);
-            M3 Ys;
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int b = 0; b < 3; ++b) Ys(a, b) = 0.5 * (Y(a, b) + Y(b, a));
-            const M3 dTs = voigt_apply(D2, Ys);
-            M3 PK = mul(dFe, t1);
-            axpy(PK, 1.0, mulNT(mul(FE_tau, dTs), t2));
-            axpy(PK, -1.0, mulNT(mul(t3, dFe), Finv));
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) PK(a, j) -= Finv(j, kk) * Z(a, l);
-#pragma unroll
-            for (int c = 0; c < 9; ++c) out.dPdF[c * 9 + kl] = out.scale * PK.a[c];
-        }
-    }
-
-    // ---- outputs and history (:942-959); CRSS/backstress are already in _iter
+    // ---- outputs and history (:942-959), written before the final tangent
+    // so that P, T and Fp are not held through it; CRSS/backstress are
+    // already in _iter
     if (out.P)
 #pragma unroll
         for (int c = 0; c < 9; ++c) out.P[c] = out.scale * P_tau.a[c];
@@ -638,6 +643,33 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         for (int c = 0; c < 9; ++c) out.T[c] = T_tau.a[c];
     store_soa3(g.Fe_i, cnt, i, FE_tau);
     store_soa3(g.Fp_i, cnt, i, FP_tau);
+    {
+        bool finite = true;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) finite = finite && isfinite(P_tau.a[c]);
+        if (!finite) status |= QP_NONFINITE;
+    }
+
+    // ---- final tangent (:835-940)
+    if (flag == 1 && out.dPdF) {
+        const bool plastic = dFp_nonzero || lazy_p > 0;
+        auto x1 = [&](int kl, M3& X1) -> bool {
+            if (!plastic) return false;
+            if (lazy_p > 0) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) {
+                    double acc = 0.0;
+                    for (int r = 0; r < lazy_p; ++r) acc += w.A[c * PMAX + r] * w.rhs[r * 9 + kl];
+                    X1.a[c] = acc;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) X1.a[c] = dFp[c * 9 + kl];
+            }
+            return true;
+        };
+        final_tangent(F, FE_tau, Fpn_inv, Tst, D2, x1, out.scale, out.dPdF);
+    }
 
     // ---- twin reorientation (:962-1019)
     if (L.twinning) {
@@ -683,10 +715,6 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         }
     }
 
-    bool finite = true;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) finite = finite && isfinite(P_tau.a[c]);
-    if (!finite) status |= QP_NONFINITE;
     if (maxcond > 1e12) status |= QP_ILL_CONDITIONED;
     if (stats_out) {
         stats_out[0] = p0 < 0 ? 0 : p0;

@@ -61,8 +61,10 @@ void run_all(const LatDev& L, const Opts& o, const GroupDev& g, const double* F,
         out.T = T ? T + 9 * i : nullptr;
         out.dPdF = (dPdF && flag == 1) ? dPdF + 81 * i : nullptr;
         out.scale = 1.0;
+        double d2[21];  // the kernel keeps this slot in shared memory
         const int st = g_variant == 0
-                           ? qp_update2<PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0)
+                           ? qp_update2<PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0,
+                                              d2, 1)
                            : qp_update<NT, PMAX>(L, o, g, i, Fk, flag, F_e, F_r, out, stats ? stats + 8 * i : nullptr, 0);
         if (status) status[i] = st;
     }
