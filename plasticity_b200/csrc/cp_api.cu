@@ -269,13 +269,22 @@ struct Group {
     int* d_perm = nullptr;           // internal qps in sorted order
     int* d_hist = nullptr;           // SORT_BUCKETS counts, then SORT_BUCKETS offsets
     GroupDev dev{};
+    std::vector<int64_t> qp_host;    // host copy of d_qp (increasing caller indices)
 };
+
+// Host-pointer updates run in caller-order chunks so that one chunk's copies
+// overlap another chunk's kernels (chunk c is a contiguous internal range of
+// every group, since each group keeps its qps in caller order).
+constexpr int MAX_CHUNKS = 4;
+int chunks_for(int64_t n) { return n >= (1 << 20) ? 4 : (n >= (1 << 18) ? 2 : 1); }
 
 }  // namespace
 
 struct cp_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t s_in = nullptr, s_out = nullptr;  // host-to-device and device-to-host copies
+    cudaEvent_t ev_in[MAX_CHUNKS] = {}, ev_done[MAX_CHUNKS] = {};
     cp_options_t opts{};
     Opts dopts{};
     int n_lat = 0;
@@ -445,36 +454,41 @@ void timing_end(cp_handle* h, int gi, cudaEvent_t a) {
     h->pending.push_back({a, b, gi});
 }
 
-// sort the group's qps by potentially-active-set size (descending)
+// Sort internal qps [i0, i0 + m) of a group by potentially-active-set size
+// (descending) into positions i0.. of its permutation.
 template <class FSrc>
-void sort_group(cp_handle* h, const Group& g, FSrc fs) {
+void sort_group(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m) {
     cudaMemsetAsync(g.d_hist, 0, sizeof(int) * SORT_BUCKETS, h->stream);
-    classify_kernel<FSrc><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], h->dopts,
-                                                                                   g.dev, fs, g.d_key, g.d_hist);
+    classify_kernel<FSrc><<<blocks_for(m, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], h->dopts, g.dev,
+                                                                             fs, i0, m, g.d_key, g.d_hist);
     bucket_scan_kernel<<<1, 32, 0, h->stream>>>(g.d_hist, g.d_hist + SORT_BUCKETS);
-    bucket_scatter_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(g.d_key, g.count, g.d_hist + SORT_BUCKETS,
-                                                                         g.d_perm);
+    bucket_scatter_kernel<<<blocks_for(m, 256), 256, 0, h->stream>>>(g.d_key, i0, m, g.d_hist + SORT_BUCKETS,
+                                                                    g.d_perm + i0);
 }
 
 template <int PMAX, class FSrc>
-void launch_update2(cp_handle* h, const Group& g, FSrc fs, int flag, double F_e, double F_r, double* P, double* T,
-                    double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
-    update2_kernel<PMAX, FSrc><<<blocks_for(g.count, UPDATE2_BLOCK), UPDATE2_BLOCK, 0, h->stream>>>(
-        h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats, kF, kT,
-        g.lattice);
+void launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m, int flag, double F_e, double F_r,
+                    double* P, double* T, double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
+    update2_kernel<PMAX, FSrc><<<blocks_for(m, UPDATE2_BLOCK), UPDATE2_BLOCK, 0, h->stream>>>(
+        h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats,
+        kF, kT, g.lattice);
 }
 
+// calculatePlasticity over internal qps [i0, i0 + m) of group gi (sort + update)
 template <class FSrc>
 void sorted_update_group(cp_handle* h, size_t gi, FSrc fs, int flag, double F_e, double F_r, double* P, double* T,
-                         double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
+                         double* dPdF, double* stage, int32_t* st, double* kF, double* kT, int64_t i0 = 0,
+                         int64_t m = -1) {
     const Group& g = h->groups[gi];
-    sort_group(h, g, fs);
+    if (m < 0) m = g.count - i0;
+    if (m <= 0) return;
+    sort_group(h, g, fs, i0, m);
     cudaEvent_t ev{};
     timing_begin(h, (int)gi, &ev);
     switch (g.nt_class) {
-        case 16: launch_update2<16>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
-        case 32: launch_update2<32>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
-        default: launch_update2<48>(h, g, fs, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+        case 16: launch_update2<16>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+        case 32: launch_update2<32>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
+        default: launch_update2<48>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
     }
     timing_end(h, (int)gi, ev);
 }
@@ -576,6 +590,15 @@ int cp_create(const cp_material_t* lattices, int32_t n_lattices, const cp_option
         delete h;
         return CP_E_CUDA;
     }
+    bool ok = cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking) == cudaSuccess;
+    for (int c = 0; ok && c < MAX_CHUNKS; ++c)
+        ok = cudaEventCreateWithFlags(&h->ev_in[c], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&h->ev_done[c], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        cp_destroy(h);
+        return CP_E_CUDA;
+    }
     h->dopts.tol = h->opts.stress_tolerance;
     h->dopts.max_search = h->opts.max_slip_search_iterations;
     h->dopts.max_solver = h->opts.max_solver_iterations;
@@ -633,6 +656,12 @@ void cp_destroy(cp_handle* h) {
         cudaEventDestroy(p.b);
     }
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->s_in) cudaStreamDestroy(h->s_in);
+    if (h->s_out) cudaStreamDestroy(h->s_out);
+    for (int c = 0; c < MAX_CHUNKS; ++c) {
+        if (h->ev_in[c]) cudaEventDestroy(h->ev_in[c]);
+        if (h->ev_done[c]) cudaEventDestroy(h->ev_done[c]);
+    }
     delete h;
 }
 
@@ -680,6 +709,7 @@ int cp_bind_qps(cp_handle* h, int64_t n_qp, const int32_t* lattice_id, const dou
             return fail(h, CP_E_NOMEM, "cp_bind_qps: device allocation failed");
         }
         CK(h, cudaMemcpy(g.d_qp, idx[l].data(), sizeof(int64_t) * g.count, cudaMemcpyHostToDevice));
+        g.qp_host = idx[l];
         carve(g);
         init_state_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(h->d_lat[l], g.dev, d_rod);
         h->groups.push_back(g);
@@ -731,17 +761,57 @@ int cp_update(cp_handle* h, const double* h_F, int32_t flag, double F_e, double 
     if (int rc = check_device(h)) return rc;
     if (int rc = ensure_staging(h, flag == 1 && h_dPdF)) return rc;
     const int64_t n = h->n_qp;
-    CK(h, cudaMemcpyAsync(h->d_F, h_F, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->stream));
     double* dd = (flag == 1 && h_dPdF) ? h->d_dPdF : nullptr;
-    if (int rc = dispatch_update(h, h->d_F, flag, F_e, F_r, h_P ? h->d_P : nullptr, h_T ? h->d_T : nullptr, dd,
-                                 h->d_status))
-        return rc;
-    if (h_P) CK(h, cudaMemcpyAsync(h_P, h->d_P, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
-    if (h_T) CK(h, cudaMemcpyAsync(h_T, h->d_T, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
-    if (dd) CK(h, cudaMemcpyAsync(h_dPdF, dd, sizeof(double) * 81 * n, cudaMemcpyDeviceToHost, h->stream));
-    if (h_status)
-        CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->stream));
+    double* dP = h_P ? h->d_P : nullptr;
+    double* dT = h_T ? h->d_T : nullptr;
+    if (h->opts.plain_kernel) {
+        CK(h, cudaMemcpyAsync(h->d_F, h_F, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->stream));
+        if (int rc = dispatch_update(h, h->d_F, flag, F_e, F_r, dP, dT, dd, h->d_status)) return rc;
+        if (h_P) CK(h, cudaMemcpyAsync(h_P, h->d_P, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+        if (h_T) CK(h, cudaMemcpyAsync(h_T, h->d_T, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
+        if (dd) CK(h, cudaMemcpyAsync(h_dPdF, dd, sizeof(double) * 81 * n, cudaMemcpyDeviceToHost, h->stream));
+        if (h_status)
+            CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        return CP_OK;
+    }
+    // chunk c: F in on s_in, the sort + update of its qps on the compute
+    // stream, its outputs out on s_out while the next chunk computes
+    double* kF = flag == 0 ? h->d_keepF : nullptr;
+    double* kT = flag == 0 ? h->d_keepT : nullptr;
+    const int C = chunks_for(n);
+    for (int c = 0; c < C; ++c) {
+        const int64_t k0 = n * c / C, k1 = n * (c + 1) / C, nk = k1 - k0;
+        CK(h, cudaMemcpyAsync(h->d_F + 9 * k0, h_F + 9 * k0, sizeof(double) * 9 * nk, cudaMemcpyHostToDevice,
+                              h->s_in));
+        CK(h, cudaEventRecord(h->ev_in[c], h->s_in));
+        CK(h, cudaStreamWaitEvent(h->stream, h->ev_in[c], 0));
+        for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+            const auto& q = h->groups[gi].qp_host;
+            const int64_t i0 = std::lower_bound(q.begin(), q.end(), k0) - q.begin();
+            const int64_t i1 = std::lower_bound(q.begin(), q.end(), k1) - q.begin();
+            sorted_update_group(h, gi, FromArray{h->d_F}, flag, F_e, F_r, dP, dT, dd, nullptr, h->d_status, kF, kT,
+                                i0, i1 - i0);
+        }
+        CK(h, cudaGetLastError());
+        CK(h, cudaEventRecord(h->ev_done[c], h->stream));
+        CK(h, cudaStreamWaitEvent(h->s_out, h->ev_done[c], 0));
+        if (h_P)
+            CK(h, cudaMemcpyAsync(h_P + 9 * k0, h->d_P + 9 * k0, sizeof(double) * 9 * nk, cudaMemcpyDeviceToHost,
+                                  h->s_out));
+        if (h_T)
+            CK(h, cudaMemcpyAsync(h_T + 9 * k0, h->d_T + 9 * k0, sizeof(double) * 9 * nk, cudaMemcpyDeviceToHost,
+                                  h->s_out));
+        if (dd)
+            CK(h, cudaMemcpyAsync(h_dPdF + 81 * k0, dd + 81 * k0, sizeof(double) * 81 * nk, cudaMemcpyDeviceToHost,
+                                  h->s_out));
+        if (h_status)
+            CK(h, cudaMemcpyAsync(h_status + k0, h->d_status + k0, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost,
+                                  h->s_out));
+    }
+    CK(h, cudaStreamSynchronize(h->s_out));
     CK(h, cudaStreamSynchronize(h->stream));
+    if (flag == 0) h->have_post = true;
     return CP_OK;
 }
 

@@ -174,14 +174,16 @@ struct FromMesh {
 constexpr int SORT_BUCKETS = 64;
 
 // sort key: bucket 63 - min(p0, 63), so ascending buckets = descending p0
+// (over internal qps [i0, i0 + m) of the group)
 template <class FSrc>
 __global__ void __launch_bounds__(QP_BLOCK) classify_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs,
-                                                            unsigned char* __restrict__ key, int* __restrict__ hist) {
+                                                            int64_t i0, int64_t m, unsigned char* __restrict__ key,
+                                                            int* __restrict__ hist) {
     __shared__ int sh[SORT_BUCKETS];
     if (threadIdx.x < SORT_BUCKETS) sh[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < g.count) {
+    const int64_t i = i0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < i0 + m) {
         const int p0 = count_potentially_active(*L, o, g, i, fs(g.qp[i]));
         const int b = SORT_BUCKETS - 1 - (p0 < SORT_BUCKETS - 1 ? p0 : SORT_BUCKETS - 1);
         key[i] = (unsigned char)b;
@@ -202,26 +204,28 @@ __global__ void bucket_scan_kernel(const int* __restrict__ hist, int* __restrict
     }
 }
 
-// scatter internal indices into bucket order (block-aggregated reservations)
-__global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char* __restrict__ key, int64_t count,
-                                                             int* __restrict__ offs, int* __restrict__ perm) {
+// scatter internal indices [i0, i0 + m) into bucket order, positions 0..m-1
+// of perm (block-aggregated reservations)
+__global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char* __restrict__ key, int64_t i0,
+                                                             int64_t m, int* __restrict__ offs,
+                                                             int* __restrict__ perm) {
     __shared__ int cnt[SORT_BUCKETS], base[SORT_BUCKETS];
     if (threadIdx.x < SORT_BUCKETS) cnt[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = i0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int b = 0, r = 0;
-    if (i < count) {
+    if (i < i0 + m) {
         b = key[i];
         r = atomicAdd(&cnt[b], 1);
     }
     __syncthreads();
     if (threadIdx.x < SORT_BUCKETS) base[threadIdx.x] = cnt[threadIdx.x] ? atomicAdd(&offs[threadIdx.x], cnt[threadIdx.x]) : 0;
     __syncthreads();
-    if (i < count) perm[base[b] + r] = (int)i;
+    if (i < i0 + m) perm[base[b] + r] = (int)i;
 }
 
-// calculatePlasticity over one group in sorted order (thread j runs internal
-// qp perm[j]).  Outputs by caller index k: P/T/dPdF/status/stats; with a
+// calculatePlasticity over m qps of one group in sorted order (thread j runs
+// internal qp perm[j]).  Outputs by caller index k: P/T/dPdF/status/stats; with a
 // non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
 // Threads run the qps in sorted order (descending potentially-active-set
 // size): consecutive threads, and so the lanes of a warp, run solves of
@@ -275,14 +279,14 @@ __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, cons
 
 template <int PMAX, class FSrc>
 __global__ void __launch_bounds__(UPDATE2_BLOCK, update2_min_blocks(PMAX))
-    update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs, const int* __restrict__ perm, int flag,
-                   double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
+    update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs, const int* __restrict__ perm, int64_t m,
+                   int flag, double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
                    double* __restrict__ stage, int32_t* __restrict__ status, int32_t* __restrict__ stats,
                    double* __restrict__ keepF, double* __restrict__ keepT, int lattice_id) {
     // per-thread rotated-stiffness slots, entry e of thread t at sD2[e * UPDATE2_BLOCK + t]
     __shared__ double sD2[21 * UPDATE2_BLOCK];
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < g.count)
+    if (j < m)
         update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
                           lattice_id, sD2 + threadIdx.x, UPDATE2_BLOCK);
 }

@@ -220,3 +220,37 @@ def test_ill_conditioned_blocks_are_flagged(oracle_lib, cuda_lib):
     agree = np.mean((st[:, 7] > 12) == (ob.stats()[:, 7] > 12))
     assert agree > 0.95, agree
     gh.close()
+
+
+@pytest.mark.parametrize("n", [(1 << 18) + 777, (1 << 20) + 123])
+def test_chunked_host_update_matches_device_update(cuda_lib, n):
+    """cp_update with host buffers runs in caller-order chunks (2 above 2^18
+    qps, 4 above 2^20) whose copies overlap the other chunks' kernels; each
+    qp's update is independent, so its outputs must equal the unchunked
+    device-pointer call's bit for bit."""
+    import torch
+    rng = np.random.default_rng(71)
+    lid = rng.choice(3, size=n, p=[0.5, 0.3, 0.2]).astype(np.int32)
+    gh = CpHandle([M.fcc_cu(), M.bcc_48(), M.hcp_mg()])
+    gh.bind_qps(lid, M.random_rodrigues(rng, n))
+    F = np.tile(np.eye(3).ravel(), (n, 1))
+    F = evolve(gh, F, rng, 3)
+    F1 = random_increment(rng, F)
+    P, T, D, st = gh.update(F1, 1)
+    s_host = gh.stats()
+    dev = torch.device("cuda", 0)
+    Fd = torch.from_numpy(F1).to(dev)
+    Pd = torch.empty(n, 9, dtype=torch.float64, device=dev)
+    Td = torch.empty(n, 9, dtype=torch.float64, device=dev)
+    Dd = torch.empty(n, 81, dtype=torch.float64, device=dev)
+    Sd = torch.empty(n, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    gh.update_device(Fd.data_ptr(), 1, 0.0, 0.0, Pd.data_ptr(), Td.data_ptr(), Dd.data_ptr(), Sd.data_ptr())
+    gh.synchronize()
+    assert np.array_equal(P, Pd.cpu().numpy())
+    assert np.array_equal(T, Td.cpu().numpy())
+    assert np.array_equal(D, Dd.cpu().numpy())
+    assert np.array_equal(st, Sd.cpu().numpy())
+    assert np.array_equal(s_host, gh.stats())
+    assert (s_host[:, 1] > 0).mean() > 0.3  # a plastic workload
+    gh.close()
