@@ -252,6 +252,61 @@ int32_t cp_field_width(const cp_handle* h, int32_t field);
 int cp_get_state(cp_handle* h, int32_t field, double* h_buf);
 int cp_set_state(cp_handle* h, int32_t field, const double* h_buf);
 
+/*
+ * The Newton step's global system on the device (next to the qp path: the
+ * reference's ellipticBVP::assemble, src/ellipticBVP/assemble.cc:62-90, with
+ * constraints.distribute_local_to_global at :78; the Dirichlet constraints of
+ * boundaryConditions.cc:453-497; solveLinearSystem.cc:10-36, PETSc BiCG with
+ * a Jacobi preconditioner and tolerance relLinearSolverTolerance * ||b||).
+ *
+ * cp_bind_dofs: after cp_bind_mesh.  h_cell_dofs holds the 24 global dof
+ * indices of every cell in local-dof order (d = 3a + c), h_constrained the
+ * Dirichlet dofs.  Builds the CSR pattern of K and, per matrix entry and per
+ * dof, the list of element entries that sum into it (cell order, so the
+ * scatter is deterministic).  The displacement u (n_dofs) starts at zero.
+ */
+int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs,
+                 int64_t n_constrained, const int64_t* h_constrained);
+int cp_set_displacement(cp_handle* h, const double* h_u);
+int cp_get_displacement(cp_handle* h, double* h_u);
+
+#define CP_SOLVER_BICG 0     /* PETScWrappers::SolverBiCG, the reference's solver */
+#define CP_SOLVER_BICGSTAB 1 /* BiCGStab (right Jacobi preconditioning) */
+typedef struct cp_solver_t {
+    int32_t kind;           /* CP_SOLVER_* */
+    int32_t max_iterations; /* "Maximum linear solver iterations" (decks: 50000) */
+    double rel_tolerance;   /* "Relative linear solver tolerance": stop at ||r|| <= tol ||b|| */
+    int32_t precond_norm;   /* 0: true residual ||b - K du||; 1: ||M^-1 r|| (PETSc's BiCG default) */
+    int32_t check_every;    /* iterations queued between host checks of convergence (0: 8) */
+} cp_solver_t;
+typedef struct cp_solve_info_t {
+    int32_t iterations; /* Krylov iterations to convergence (or the cap) */
+    int32_t converged;  /* 1 if the tolerance was met */
+    int32_t breakdown;  /* 1 if the method broke down (zero rho or denominator) */
+    int32_t reserved;
+    double rhs_norm;      /* ||b|| of the condensed system */
+    double residual_norm; /* the tested residual norm at exit */
+} cp_solve_info_t;
+int cp_solver_default(cp_solver_t* solver); /* BiCG, 50000, 1e-10, true residual */
+
+/*
+ * One Newton iteration on the device (solveNonLinearSystem.cc:14-81, one
+ * pass): U_local gathered from u, batched getElementalValues, K and R
+ * scattered, the constrained dofs' increments h_du_constrained (n_constrained
+ * values in cp_bind_dofs order; NULL = zero) condensed into the system, the
+ * Krylov solve, constrained dofs set to their increments (distribute), and
+ * u += du.  solver NULL = cp_solver_default.  info may be NULL.
+ */
+int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
+                        const cp_solver_t* solver, cp_solve_info_t* info);
+
+/*
+ * The post-pass calculatePlasticity(...,0) at every qp
+ * (updateAfterIncrement.cc:105) with F from the device displacement; then
+ * cp_averages / cp_reorient / cp_commit as after cp_update.
+ */
+int cp_update_from_displacement(cp_handle* h, double F_e, double F_r);
+
 /* Wait for all work queued on the handle's stream. */
 int cp_synchronize(cp_handle* h);
 

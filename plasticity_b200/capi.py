@@ -84,6 +84,42 @@ class CpOptions(C.Structure):
     ]
 
 
+class CpSolver(C.Structure):
+    """cp_solver_t: the Newton step's Krylov solve (solveLinearSystem.cc:10-36)."""
+
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("max_iterations", C.c_int32),
+        ("rel_tolerance", C.c_double),
+        ("precond_norm", C.c_int32),
+        ("check_every", C.c_int32),
+    ]
+
+
+class CpSolveInfo(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("breakdown", C.c_int32),
+        ("reserved", C.c_int32),
+        ("rhs_norm", C.c_double),
+        ("residual_norm", C.c_double),
+    ]
+
+
+CP_SOLVER_BICG = 0
+CP_SOLVER_BICGSTAB = 1
+
+
+def default_solver(**kw) -> CpSolver:
+    """The reference decks' settings: BiCG, 50000 iterations, 1e-10 x ||b||."""
+    s = CpSolver()
+    s.kind, s.max_iterations, s.rel_tolerance, s.precond_norm, s.check_every = CP_SOLVER_BICG, 50000, 1e-10, 0, 8
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
 def default_options(**kw) -> CpOptions:
     """The reference's shipped values: Stress Tolerance 1e-9, caps 1/1."""
     o = CpOptions()
@@ -141,6 +177,13 @@ def load_library(path: str | None = None) -> C.CDLL:
     H = C.c_void_p
     sig = {
         "cp_options_default": (C.c_int, [C.POINTER(CpOptions)]),
+        "cp_bind_dofs": (C.c_int, [H, I64, C.POINTER(C.c_int64), I64, C.POINTER(C.c_int64)]),
+        "cp_set_displacement": (C.c_int, [H, D]),
+        "cp_get_displacement": (C.c_int, [H, D]),
+        "cp_solver_default": (C.c_int, [C.POINTER(CpSolver)]),
+        "cp_newton_iteration": (C.c_int, [H, D, C.c_double, C.c_double, C.POINTER(CpSolver),
+                                          C.POINTER(CpSolveInfo)]),
+        "cp_update_from_displacement": (C.c_int, [H, C.c_double, C.c_double]),
         "cp_material_add_dummy_twin": (C.c_int, [C.POINTER(CpMaterial)]),
         "cp_create": (C.c_int, [C.POINTER(CpMaterial), C.c_int32, C.POINTER(CpOptions), C.POINTER(H)]),
         "cp_destroy": (None, [H]),
@@ -277,6 +320,37 @@ class CpHandle:
         out = np.empty(22)
         self._check(self.lib.cp_averages(self.h, dptr(out)), "cp_averages")
         return out
+
+    # ---- the Newton step's global system on the device
+    def bind_dofs(self, n_dofs: int, cell_dofs, constrained):
+        cd = np.ascontiguousarray(cell_dofs, dtype=np.int64).reshape(-1)
+        con = np.ascontiguousarray(constrained, dtype=np.int64).reshape(-1)
+        p64 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        self._check(self.lib.cp_bind_dofs(self.h, int(n_dofs), p64(cd), len(con), p64(con) if len(con) else None),
+                    "cp_bind_dofs")
+        self.n_dofs = int(n_dofs)
+
+    def set_displacement(self, u):
+        u = as_f64(u, (self.n_dofs,))
+        self._check(self.lib.cp_set_displacement(self.h, dptr(u)), "cp_set_displacement")
+
+    def get_displacement(self):
+        u = np.empty(self.n_dofs)
+        self._check(self.lib.cp_get_displacement(self.h, dptr(u)), "cp_get_displacement")
+        return u
+
+    def newton_iteration(self, du_constrained=None, F_e: float = 0.0, F_r: float = 0.0, solver: CpSolver | None = None):
+        """One device Newton pass (assemble, scatter, condense, solve, u += du); returns the solve info."""
+        duc = None if du_constrained is None else as_f64(du_constrained)
+        info = CpSolveInfo()
+        self._check(self.lib.cp_newton_iteration(self.h, dptr(duc), F_e, F_r,
+                                                 C.byref(solver) if solver is not None else None,
+                                                 C.byref(info)), "cp_newton_iteration")
+        return {"iterations": info.iterations, "converged": bool(info.converged), "breakdown": bool(info.breakdown),
+                "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
+
+    def update_from_displacement(self, F_e: float = 0.0, F_r: float = 0.0):
+        self._check(self.lib.cp_update_from_displacement(self.h, F_e, F_r), "cp_update_from_displacement")
 
     def reorient(self):
         self._check(self.lib.cp_reorient(self.h), "cp_reorient")

@@ -11,6 +11,7 @@
 
 #include "../../include/cp_gpu.h"
 #include "cp_kernels.cuh"
+#include "cp_solve.cuh"
 
 using namespace cp;
 
@@ -307,6 +308,23 @@ struct cp_handle {
     double *d_gradN = nullptr, *d_JxW = nullptr;
     double *d_U = nullptr, *d_Ke = nullptr, *d_Re = nullptr;
     double* d_stage = nullptr;  // JxW*P and JxW*dP/dF per qp between update and contraction
+    // global system of the Newton step (cp_bind_dofs)
+    struct System {
+        int64_t n_dofs = 0, nnz = 0, n_con = 0;
+        int64_t* d_cell_dofs = nullptr;         // 24 per cell
+        int64_t* d_row_ptr = nullptr;           // n_dofs + 1
+        int* d_col = nullptr;                   // nnz
+        int64_t* d_tpos = nullptr;              // nnz: position of the transposed entry
+        int64_t* d_diag = nullptr;              // n_dofs: position of the diagonal entry
+        int64_t *d_kptr = nullptr, *d_kidx = nullptr;  // element-matrix contributions per entry
+        int64_t *d_rptr = nullptr, *d_ridx = nullptr;  // element-residual contributions per dof
+        int64_t* d_con = nullptr;               // constrained dofs
+        unsigned char* d_cmask = nullptr;       // n_dofs
+        double *d_vals = nullptr, *d_Ke = nullptr, *d_Re = nullptr, *d_Ul = nullptr, *d_duc = nullptr;
+        double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
+        double *d_sc = nullptr, *d_partial = nullptr;
+        int *d_done = nullptr, *d_info = nullptr;
+    } sys;
     // averages scratch
     double *d_avg_partial = nullptr, *d_avg_out = nullptr;
     int64_t avg_cap = 0;
@@ -371,7 +389,10 @@ void free_qps(cp_handle* h) {
     h->have_post = false;
 }
 
+void free_system(cp_handle* h);
+
 void free_mesh(cp_handle* h) {
+    free_system(h);
     cudaFree(h->d_gradN);
     cudaFree(h->d_JxW);
     cudaFree(h->d_U);
@@ -380,6 +401,36 @@ void free_mesh(cp_handle* h) {
     cudaFree(h->d_stage);
     h->d_gradN = h->d_JxW = h->d_U = h->d_Ke = h->d_Re = h->d_stage = nullptr;
     h->n_cells = 0;
+}
+
+// vectors of the Newton system, n_dofs doubles each, in d_vec
+enum SysVec { V_U = 0, V_X, V_R, V_RHS, V_DC, V_KDC, V_RES, V_RT, V_Z, V_ZT, V_P, V_PT, V_Q, V_QT, V_DINV, V_S, V_T,
+              V_PH, V_SH, SYS_VECS };
+
+void free_system(cp_handle* h) {
+    auto& y = h->sys;
+    cudaFree(y.d_cell_dofs);
+    cudaFree(y.d_row_ptr);
+    cudaFree(y.d_col);
+    cudaFree(y.d_tpos);
+    cudaFree(y.d_diag);
+    cudaFree(y.d_kptr);
+    cudaFree(y.d_kidx);
+    cudaFree(y.d_rptr);
+    cudaFree(y.d_ridx);
+    cudaFree(y.d_con);
+    cudaFree(y.d_cmask);
+    cudaFree(y.d_vals);
+    cudaFree(y.d_Ke);
+    cudaFree(y.d_Re);
+    cudaFree(y.d_Ul);
+    cudaFree(y.d_duc);
+    cudaFree(y.d_vec);
+    cudaFree(y.d_sc);
+    cudaFree(y.d_partial);
+    cudaFree(y.d_done);
+    cudaFree(y.d_info);
+    y = cp_handle::System{};
 }
 
 // double fields of a group in the order they are carved out of d_block
@@ -1178,6 +1229,334 @@ int cp_synchronize(cp_handle* h) {
     if (!h) return CP_E_ARG;
     if (int rc = check_device(h)) return rc;
     CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+// ---- the Newton step's global system ------------------------------------
+
+int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64_t n_constrained,
+                 const int64_t* h_constrained) {
+    if (!h) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_bind_dofs: no mesh bound");
+    if (n_dofs < 1 || n_dofs > INT32_MAX || !h_cell_dofs || n_constrained < 0 || (n_constrained && !h_constrained))
+        return fail(h, CP_E_ARG, "cp_bind_dofs: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    const int64_t nc = h->n_cells;
+    for (int64_t t = 0; t < 24 * nc; ++t)
+        if (h_cell_dofs[t] < 0 || h_cell_dofs[t] >= n_dofs)
+            return fail(h, CP_E_ARG, "cp_bind_dofs: dof index out of range");
+    for (int64_t c = 0; c < nc; ++c)
+        for (int a = 0; a < 24; ++a)
+            for (int b = a + 1; b < 24; ++b)
+                if (h_cell_dofs[24 * c + a] == h_cell_dofs[24 * c + b])
+                    return fail(h, CP_E_ARG, "cp_bind_dofs: repeated dof within a cell");
+    std::vector<unsigned char> cmask(n_dofs, 0);
+    for (int64_t j = 0; j < n_constrained; ++j) {
+        if (h_constrained[j] < 0 || h_constrained[j] >= n_dofs)
+            return fail(h, CP_E_ARG, "cp_bind_dofs: constrained dof out of range");
+        if (cmask[h_constrained[j]]) return fail(h, CP_E_ARG, "cp_bind_dofs: constrained dof listed twice");
+        cmask[h_constrained[j]] = 1;
+    }
+    // CSR pattern: row i holds the dofs of every cell that holds i
+    std::vector<int64_t> row_ptr(n_dofs + 1, 0);
+    for (int64_t t = 0; t < 24 * nc; ++t) row_ptr[h_cell_dofs[t] + 1] += 24;
+    for (int64_t i = 0; i < n_dofs; ++i) row_ptr[i + 1] += row_ptr[i];
+    std::vector<int> cand(row_ptr[n_dofs]);
+    {
+        std::vector<int64_t> fill(row_ptr.begin(), row_ptr.end() - 1);
+        for (int64_t c = 0; c < nc; ++c)
+            for (int a = 0; a < 24; ++a) {
+                const int64_t i = h_cell_dofs[24 * c + a];
+                for (int b = 0; b < 24; ++b) cand[fill[i]++] = (int)h_cell_dofs[24 * c + b];
+            }
+    }
+    std::vector<int64_t> rp(n_dofs + 1, 0);
+    std::vector<int> col;
+    col.reserve(cand.size() / 2);
+    for (int64_t i = 0; i < n_dofs; ++i) {
+        auto b = cand.begin() + row_ptr[i], e = cand.begin() + row_ptr[i + 1];
+        std::sort(b, e);
+        e = std::unique(b, e);
+        col.insert(col.end(), b, e);
+        rp[i + 1] = (int64_t)col.size();
+    }
+    const int64_t nnz = (int64_t)col.size();
+    auto find = [&](int64_t i, int j) -> int64_t {
+        const auto b = col.begin() + rp[i], e = col.begin() + rp[i + 1];
+        return (int64_t)(std::lower_bound(b, e, j) - col.begin());
+    };
+    std::vector<int64_t> tpos(nnz), diag(n_dofs);
+    for (int64_t i = 0; i < n_dofs; ++i) {
+        diag[i] = rp[i + 1] > rp[i] ? find(i, (int)i) : -1;
+        for (int64_t p = rp[i]; p < rp[i + 1]; ++p) tpos[p] = find(col[p], (int)i);
+    }
+    for (int64_t i = 0; i < n_dofs; ++i)
+        if (diag[i] < 0) return fail(h, CP_E_ARG, "cp_bind_dofs: a dof belongs to no cell");
+    // contributions of element entries (cell order within each entry)
+    std::vector<int64_t> kptr(nnz + 1, 0), kidx(576 * nc), epos(576 * nc);
+    for (int64_t c = 0; c < nc; ++c)
+        for (int a = 0; a < 24; ++a)
+            for (int b = 0; b < 24; ++b) {
+                const int64_t p = find(h_cell_dofs[24 * c + a], (int)h_cell_dofs[24 * c + b]);
+                epos[576 * c + 24 * a + b] = p;
+                kptr[p + 1] += 1;
+            }
+    for (int64_t p = 0; p < nnz; ++p) kptr[p + 1] += kptr[p];
+    {
+        std::vector<int64_t> fill(kptr.begin(), kptr.end() - 1);
+        for (int64_t e = 0; e < 576 * nc; ++e) kidx[fill[epos[e]]++] = e;
+    }
+    std::vector<int64_t> rptr(n_dofs + 1, 0), ridx(24 * nc);
+    for (int64_t t = 0; t < 24 * nc; ++t) rptr[h_cell_dofs[t] + 1] += 1;
+    for (int64_t i = 0; i < n_dofs; ++i) rptr[i + 1] += rptr[i];
+    {
+        std::vector<int64_t> fill(rptr.begin(), rptr.end() - 1);
+        for (int64_t t = 0; t < 24 * nc; ++t) ridx[fill[h_cell_dofs[t]]++] = t;
+    }
+    free_system(h);
+    auto& y = h->sys;
+    y.n_dofs = n_dofs;
+    y.nnz = nnz;
+    y.n_con = n_constrained;
+    bool ok = cudaMalloc(&y.d_cell_dofs, sizeof(int64_t) * 24 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_row_ptr, sizeof(int64_t) * (n_dofs + 1)) == cudaSuccess &&
+              cudaMalloc(&y.d_col, sizeof(int) * nnz) == cudaSuccess &&
+              cudaMalloc(&y.d_tpos, sizeof(int64_t) * nnz) == cudaSuccess &&
+              cudaMalloc(&y.d_diag, sizeof(int64_t) * n_dofs) == cudaSuccess &&
+              cudaMalloc(&y.d_kptr, sizeof(int64_t) * (nnz + 1)) == cudaSuccess &&
+              cudaMalloc(&y.d_kidx, sizeof(int64_t) * 576 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_rptr, sizeof(int64_t) * (n_dofs + 1)) == cudaSuccess &&
+              cudaMalloc(&y.d_ridx, sizeof(int64_t) * 24 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_con, sizeof(int64_t) * std::max<int64_t>(n_constrained, 1)) == cudaSuccess &&
+              cudaMalloc(&y.d_cmask, n_dofs) == cudaSuccess &&
+              cudaMalloc(&y.d_vals, sizeof(double) * nnz) == cudaSuccess &&
+              cudaMalloc(&y.d_Ke, sizeof(double) * 576 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_Re, sizeof(double) * 24 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_Ul, sizeof(double) * 24 * nc) == cudaSuccess &&
+              cudaMalloc(&y.d_duc, sizeof(double) * std::max<int64_t>(n_constrained, 1)) == cudaSuccess &&
+              cudaMalloc(&y.d_vec, sizeof(double) * SYS_VECS * n_dofs) == cudaSuccess &&
+              cudaMalloc(&y.d_sc, sizeof(double) * SC_COUNT) == cudaSuccess &&
+              cudaMalloc(&y.d_partial, sizeof(double) * RED_BLOCKS) == cudaSuccess &&
+              cudaMalloc(&y.d_done, sizeof(int)) == cudaSuccess && cudaMalloc(&y.d_info, sizeof(int) * 3) == cudaSuccess;
+    if (!ok) {
+        free_system(h);
+        return fail(h, CP_E_NOMEM, "cp_bind_dofs: device allocation failed");
+    }
+    CK(h, cudaMemcpy(y.d_cell_dofs, h_cell_dofs, sizeof(int64_t) * 24 * nc, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_row_ptr, rp.data(), sizeof(int64_t) * (n_dofs + 1), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_col, col.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_tpos, tpos.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_diag, diag.data(), sizeof(int64_t) * n_dofs, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_kptr, kptr.data(), sizeof(int64_t) * (nnz + 1), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_kidx, kidx.data(), sizeof(int64_t) * 576 * nc, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_rptr, rptr.data(), sizeof(int64_t) * (n_dofs + 1), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_ridx, ridx.data(), sizeof(int64_t) * 24 * nc, cudaMemcpyHostToDevice));
+    if (n_constrained)
+        CK(h, cudaMemcpy(y.d_con, h_constrained, sizeof(int64_t) * n_constrained, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(y.d_cmask, cmask.data(), n_dofs, cudaMemcpyHostToDevice));
+    CK(h, cudaMemset(y.d_vec, 0, sizeof(double) * SYS_VECS * n_dofs));
+    return CP_OK;
+}
+
+int cp_set_displacement(cp_handle* h, const double* h_u) {
+    if (!h || !h_u) return CP_E_ARG;
+    if (!h->sys.n_dofs) return fail(h, CP_E_STATE, "cp_set_displacement: no dofs bound");
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaMemcpyAsync(h->sys.d_vec + V_U * h->sys.n_dofs, h_u, sizeof(double) * h->sys.n_dofs,
+                          cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+int cp_get_displacement(cp_handle* h, double* h_u) {
+    if (!h || !h_u) return CP_E_ARG;
+    if (!h->sys.n_dofs) return fail(h, CP_E_STATE, "cp_get_displacement: no dofs bound");
+    if (int rc = check_device(h)) return rc;
+    CK(h, cudaMemcpyAsync(h_u, h->sys.d_vec + V_U * h->sys.n_dofs, sizeof(double) * h->sys.n_dofs,
+                          cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return CP_OK;
+}
+
+namespace {
+
+// a = sum_i x_i y_i into sc[slot] (deterministic two-stage)
+void sys_dot(cp_handle* h, const double* x, const double* y, int slot, const int* done) {
+    auto& s = h->sys;
+    dot_partial_kernel<<<RED_BLOCKS, SOLVE_BLOCK, 0, h->stream>>>(x, y, s.n_dofs, s.d_partial, done);
+    dot_final_kernel<<<1, SOLVE_BLOCK, 0, h->stream>>>(s.d_partial, s.d_sc + slot, done);
+}
+
+void sys_spmv(cp_handle* h, const double* x, double* y, bool transpose, const int* done) {
+    auto& s = h->sys;
+    const int64_t threads = 32 * s.n_dofs;
+    spmv_kernel<<<blocks_for(threads, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+        s.d_row_ptr, s.d_col, s.d_vals, transpose ? s.d_tpos : nullptr, x, s.n_dofs, y, done);
+}
+
+// one Krylov iteration of the chosen method (queued, no host sync)
+void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
+    auto& s = h->sys;
+    const int64_t n = s.n_dofs;
+    const unsigned nb = blocks_for(n, SOLVE_BLOCK);
+    double* V = s.d_vec;
+    auto v = [&](int k) { return V + (int64_t)k * n; };
+    const int* done = s.d_done;
+    if (sv.kind == CP_SOLVER_BICGSTAB) {
+        sys_dot(h, v(V_RT), v(V_RES), SC_RHO, done);
+        bicgstab_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_RES), v(V_Q), n, first, v(V_P),
+                                                                 s.d_done, s.d_info);
+        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_P), v(V_DINV), n, v(V_PH), done);
+        sys_spmv(h, v(V_PH), v(V_Q), false, done);  // v
+        sys_dot(h, v(V_RT), v(V_Q), SC_DEN, done);
+        bicgstab_s_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_RES), v(V_Q), n, v(V_S), s.d_done,
+                                                               s.d_info);
+        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_S), v(V_DINV), n, v(V_SH), done);
+        sys_spmv(h, v(V_SH), v(V_T), false, done);
+        sys_dot(h, v(V_T), v(V_S), SC_TS, done);
+        sys_dot(h, v(V_T), v(V_T), SC_TT, done);
+        bicgstab_x_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_PH), v(V_SH), v(V_S), v(V_T), n, v(V_X),
+                                                               v(V_RES), done);
+    } else {
+        jacobi2_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_DINV), v(V_RES), v(V_RT), n, v(V_Z), v(V_ZT), done);
+        sys_dot(h, v(V_Z), v(V_RT), SC_RHO, done);
+        bicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
+                                                             s.d_done, s.d_info);
+        sys_spmv(h, v(V_P), v(V_Q), false, done);
+        sys_spmv(h, v(V_PT), v(V_QT), true, done);
+        sys_dot(h, v(V_PT), v(V_Q), SC_DEN, done);
+        bicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_P), v(V_Q), v(V_QT), n, v(V_X), v(V_RES),
+                                                              v(V_RT), s.d_done, s.d_info);
+    }
+    sys_dot(h, v(V_RES), v(V_RES), SC_RR, done);
+    if (sv.precond_norm) {
+        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RES), v(V_DINV), n, v(V_Z), done);
+        sys_dot(h, v(V_Z), v(V_Z), SC_ZZ, done);
+    }
+    check_kernel<<<1, 1, 0, h->stream>>>(s.d_sc, sv.rel_tolerance, sv.precond_norm, s.d_done, s.d_info);
+    shift_rho_kernel<<<1, 1, 0, h->stream>>>(s.d_sc, done);
+}
+
+}  // namespace
+
+int cp_solver_default(cp_solver_t* sv) {
+    if (!sv) return CP_E_ARG;
+    sv->kind = CP_SOLVER_BICG;
+    sv->max_iterations = 50000;
+    sv->rel_tolerance = 1.0e-10;
+    sv->precond_norm = 0;
+    sv->check_every = 8;
+    return CP_OK;
+}
+
+int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
+                        const cp_solver_t* solver, cp_solve_info_t* info) {
+    if (!h) return CP_E_ARG;
+    auto& s = h->sys;
+    if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_newton_iteration: no dofs bound");
+    cp_solver_t sv;
+    if (solver)
+        sv = *solver;
+    else
+        cp_solver_default(&sv);
+    if ((sv.kind != CP_SOLVER_BICG && sv.kind != CP_SOLVER_BICGSTAB) || sv.max_iterations < 1 ||
+        !(sv.rel_tolerance >= 0.0))
+        return fail(h, CP_E_ARG, "cp_newton_iteration: bad solver settings");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    const int64_t n = s.n_dofs, nc = h->n_cells;
+    double* V = s.d_vec;
+    auto v = [&](int k) { return V + (int64_t)k * n; };
+    const unsigned nb = blocks_for(n, SOLVE_BLOCK);
+    // batched getElementalValues at the current u
+    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(v(V_U), s.d_cell_dofs,
+                                                                                         24 * nc, s.d_Ul);
+    if (int rc = cp_assemble_device(h, s.d_Ul, F_e, F_r, s.d_Ke, s.d_Re, h->d_status)) return rc;
+    // K and R (distribute_local_to_global), in cell order per entry
+    scatter_sum_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_Ke, s.d_kptr, s.d_kidx,
+                                                                                     s.nnz, s.d_vals);
+    scatter_sum_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_Re, s.d_rptr, s.d_ridx, n, v(V_R));
+    // condensation of the prescribed increments
+    if (s.n_con && h_du_constrained)
+        CK(h, cudaMemcpyAsync(s.d_duc, h_du_constrained, sizeof(double) * s.n_con, cudaMemcpyHostToDevice,
+                              h->stream));
+    const double* duc = (s.n_con && h_du_constrained) ? s.d_duc : nullptr;
+    CK(h, cudaMemsetAsync(v(V_DC), 0, sizeof(double) * n, h->stream));
+    if (s.n_con)
+        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
+                                                                                                  s.n_con, v(V_DC));
+    sys_spmv(h, v(V_DC), v(V_KDC), false, nullptr);
+    condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
+    condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
+    jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
+    // Krylov solve from x = 0: r = r~ = rhs
+    CK(h, cudaMemsetAsync(v(V_X), 0, sizeof(double) * n, h->stream));
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(V_RES));
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(V_RT));
+    CK(h, cudaMemsetAsync(s.d_done, 0, sizeof(int), h->stream));
+    CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
+    CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
+    sys_dot(h, v(V_RHS), v(V_RHS), SC_BB, nullptr);
+    sys_dot(h, v(V_RHS), v(V_RHS), SC_RR, nullptr);
+    if (sv.precond_norm) {
+        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), v(V_DINV), n, v(V_Z), nullptr);
+        sys_dot(h, v(V_Z), v(V_Z), SC_ZZ, nullptr);
+    }
+    double sc0[SC_COUNT];
+    CK(h, cudaMemcpyAsync(sc0, s.d_sc, sizeof sc0, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    int hinfo[3] = {0, 0, 0};
+    const double bnorm = std::sqrt(sc0[SC_BB]);
+    if (bnorm == 0.0) {
+        hinfo[1] = 1;  // du = 0 solves it
+    } else {
+        const int every = sv.check_every > 0 ? sv.check_every : 8;
+        int queued = 0;
+        while (queued < sv.max_iterations) {
+            const int k = std::min(every, sv.max_iterations - queued);
+            for (int t = 0; t < k; ++t) krylov_iteration(h, sv, queued + t == 0);
+            queued += k;
+            CK(h, cudaGetLastError());
+            CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof hinfo, cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaStreamSynchronize(h->stream));
+            if (hinfo[1] || hinfo[2]) break;
+        }
+    }
+    // distribute: constrained dofs take their prescribed increments exactly
+    if (s.n_con)
+        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
+                                                                                                  s.n_con, v(V_X));
+    add_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_X), n, v(V_U));
+    CK(h, cudaGetLastError());
+    double scf[SC_COUNT];
+    CK(h, cudaMemcpyAsync(scf, s.d_sc, sizeof scf, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (info) {
+        info->iterations = hinfo[0];
+        info->converged = hinfo[1];
+        info->breakdown = hinfo[2];
+        info->rhs_norm = bnorm;
+        info->residual_norm = bnorm == 0.0 ? 0.0 : std::sqrt(sv.precond_norm ? scf[SC_ZZ] : scf[SC_RR]);
+    }
+    return CP_OK;
+}
+
+int cp_update_from_displacement(cp_handle* h, double F_e, double F_r) {
+    if (!h) return CP_E_ARG;
+    auto& s = h->sys;
+    if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_update_from_displacement: no dofs bound");
+    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_update_from_displacement: needs the sorted update");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    const int64_t nc = h->n_cells;
+    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+        s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
+    const FromMesh fm{s.d_Ul, h->d_gradN, h->d_JxW, h->uniform};
+    for (size_t gi = 0; gi < h->groups.size(); ++gi)
+        sorted_update_group(h, gi, fm, 0, F_e, F_r, nullptr, nullptr, nullptr, nullptr, h->d_status, h->d_keepF,
+                            h->d_keepT);
+    CK(h, cudaGetLastError());
+    h->have_post = true;
     return CP_OK;
 }
 

@@ -1,0 +1,308 @@
+// cp_solve.cuh -- the Newton step's global system on the device: scatter of
+// the element matrices and residuals into one CSR matrix and vector
+// (ellipticBVP::assemble, src/ellipticBVP/assemble.cc:62-90, through
+// constraints.distribute_local_to_global, :78), Dirichlet condensation
+// (boundaryConditions.cc:453-497 / AffineConstraints with inhomogeneities) and
+// the Jacobi-preconditioned Krylov solve of solveLinearSystem.cc:10-36
+// (PETScWrappers::SolverBiCG + PreconditionJacobi), restated as plain CUDA.
+//
+// Layout: K is CSR (row_ptr int64, col int32, values FP64), rows = global dofs.
+// The Q1 pattern is structurally symmetric, so tpos[p] (the position of entry
+// (j, i) for entry p = (i, j)) gives K^T products from the same arrays.  Every
+// reduction is two-stage with a fixed block count and a fixed final order, so
+// a solve is deterministic for a given input.
+#pragma once
+
+#include <cstdint>
+
+namespace cp {
+
+constexpr int SOLVE_BLOCK = 256;
+constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs
+
+// ---- gather / scatter ----------------------------------------------------
+
+// U_local[24 c + d] = u[cell_dofs[24 c + d]]  (getElementalValues.cc:31-33)
+__global__ void gather_ulocal_kernel(const double* __restrict__ u, const int64_t* __restrict__ cell_dofs,
+                                     int64_t n, double* __restrict__ Ul) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) Ul[t] = u[cell_dofs[t]];
+}
+
+// value p of the global matrix = sum of its element entries, in cell order:
+// src[idx[ptr[p]..ptr[p+1])] (element entry index cell*576 + 24 d1 + d2, or
+// cell*24 + d for the residual)
+__global__ void scatter_sum_kernel(const double* __restrict__ src, const int64_t* __restrict__ ptr,
+                                   const int64_t* __restrict__ idx, int64_t n, double* __restrict__ out) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    double s = 0.0;
+    for (int64_t q = ptr[p]; q < ptr[p + 1]; ++q) s += src[idx[q]];
+    out[p] = s;
+}
+
+// ---- condensation --------------------------------------------------------
+
+// x[con[j]] = v[j] (v null: zero); the other entries are left as they are
+__global__ void constrained_vector_kernel(const int64_t* __restrict__ con, const double* __restrict__ v,
+                                          int64_t n_con, double* __restrict__ x) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n_con) x[con[j]] = v ? v[j] : 0.0;
+}
+
+// rows and columns of constrained dofs become those of the identity
+// (du = the prescribed increment there); rhs of a constrained row = its value
+__global__ void condense_matrix_kernel(const int64_t* __restrict__ row_ptr, const int* __restrict__ col,
+                                       const unsigned char* __restrict__ cmask, int64_t n, double* __restrict__ vals) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool ci = cmask[i];
+    for (int64_t p = row_ptr[i]; p < row_ptr[i + 1]; ++p) {
+        const int j = col[p];
+        if (ci || cmask[j]) vals[p] = (ci && j == i) ? 1.0 : 0.0;
+    }
+}
+
+// rhs = R - K dc on free rows, dc on constrained rows (K still unmodified)
+__global__ void condense_rhs_kernel(const double* __restrict__ R, const double* __restrict__ Kdc,
+                                    const double* __restrict__ dc, const unsigned char* __restrict__ cmask, int64_t n,
+                                    double* __restrict__ rhs) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rhs[i] = cmask[i] ? dc[i] : R[i] - Kdc[i];
+}
+
+// ---- sparse products (a warp per row: the row's entries load coalesced) ---
+
+// y = K x, or y = K^T x when tpos is given (entry (j,i) of row i at tpos[p])
+__global__ void spmv_kernel(const int64_t* __restrict__ row_ptr, const int* __restrict__ col,
+                            const double* __restrict__ vals, const int64_t* __restrict__ tpos,
+                            const double* __restrict__ x, int64_t n, double* __restrict__ y,
+                            const int* __restrict__ done) {
+    if (done && *done) return;
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0.0;
+    for (int64_t p = row_ptr[row] + lane; p < row_ptr[row + 1]; p += 32)
+        s += (tpos ? vals[tpos[p]] : vals[p]) * x[col[p]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[row] = s;
+}
+
+// ---- reductions ------------------------------------------------------------
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[SOLVE_BLOCK / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < SOLVE_BLOCK / 32; ++w) s += sh[w];
+    __syncthreads();
+    return s;  // valid in thread 0
+}
+
+// partial[b] = sum over the block's grid-stride share of a[i] * b[i]
+__global__ void __launch_bounds__(SOLVE_BLOCK) dot_partial_kernel(const double* __restrict__ a,
+                                                                  const double* __restrict__ b, int64_t n,
+                                                                  double* __restrict__ partial,
+                                                                  const int* __restrict__ done) {
+    if (done && *done) return;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// out = sum of the RED_BLOCKS partials in a fixed order (one block)
+__global__ void __launch_bounds__(SOLVE_BLOCK) dot_final_kernel(const double* __restrict__ partial,
+                                                                double* __restrict__ out,
+                                                                const int* __restrict__ done) {
+    if (done && *done) return;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < RED_BLOCKS; i += blockDim.x) s += partial[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// ---- Krylov scalars and vector updates -------------------------------------
+//
+// Device scalars of one solve (sc[]):
+enum SolveScalar {
+    SC_RHO = 0,      // current rho
+    SC_RHO_OLD,      // previous rho
+    SC_DEN,          // p~ . q (BiCG) / r0 . v (BiCGStab)
+    SC_RR,           // ||r||^2
+    SC_BB,           // ||b||^2
+    SC_ALPHA,
+    SC_BETA,
+    SC_OMEGA,        // BiCGStab
+    SC_TS,           // t . s (BiCGStab)
+    SC_TT,           // t . t (BiCGStab)
+    SC_ZZ,           // ||M^-1 r||^2 (preconditioned norm)
+    SC_COUNT
+};
+
+// info[]: 0 iterations done, 1 converged, 2 breakdown
+// Convergence test after an iteration: ||r|| <= tol ||b|| (true residual), or
+// ||M^-1 r|| <= tol ||b|| when precond_norm (the norm PETSc's BiCG tests).
+__global__ void check_kernel(double* __restrict__ sc, double tol, int precond_norm, int* __restrict__ done,
+                             int* __restrict__ info) {
+    if (*done) return;
+    info[0] += 1;
+    const double rn = sqrt(precond_norm ? sc[SC_ZZ] : sc[SC_RR]);
+    if (rn <= tol * sqrt(sc[SC_BB])) {
+        info[1] = 1;
+        *done = 1;
+    }
+}
+
+// z = r / d, z~ = r~ / d  (Jacobi: M = diag K)
+__global__ void jacobi2_kernel(const double* __restrict__ dinv, const double* __restrict__ r,
+                               const double* __restrict__ rt, int64_t n, double* __restrict__ z,
+                               double* __restrict__ zt, const int* __restrict__ done) {
+    if (*done) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    z[i] = r[i] * dinv[i];
+    if (zt) zt[i] = rt[i] * dinv[i];
+}
+
+// BiCG direction update: p = z + beta p, p~ = z~ + beta p~ (beta = rho / rho_old; first: beta = 0)
+__global__ void bicg_dir_kernel(double* __restrict__ sc, const double* __restrict__ z,
+                                const double* __restrict__ zt, int64_t n, int first, double* __restrict__ p,
+                                double* __restrict__ pt, int* __restrict__ done, int* __restrict__ info) {
+    if (*done) return;
+    const double rho = sc[SC_RHO];
+    if (rho == 0.0 || !isfinite(rho)) {  // breakdown: stop (thread-uniform decision)
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double beta = first ? 0.0 : rho / sc[SC_RHO_OLD];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p[i] = z[i] + beta * p[i];
+    pt[i] = zt[i] + beta * pt[i];
+}
+
+// x += alpha p; r -= alpha q; r~ -= alpha q~  (alpha = rho / (p~ . q))
+__global__ void bicg_step_kernel(double* __restrict__ sc, const double* __restrict__ p, const double* __restrict__ q,
+                                 const double* __restrict__ qt, int64_t n, double* __restrict__ x,
+                                 double* __restrict__ r, double* __restrict__ rt, int* __restrict__ done,
+                                 int* __restrict__ info) {
+    if (*done) return;
+    const double den = sc[SC_DEN];
+    if (den == 0.0 || !isfinite(den)) {  // breakdown (thread-uniform decision)
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double alpha = sc[SC_RHO] / den;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] += alpha * p[i];
+    r[i] -= alpha * q[i];
+    rt[i] -= alpha * qt[i];
+}
+
+// scalar bookkeeping between iterations: rho_old = rho
+__global__ void shift_rho_kernel(double* __restrict__ sc, const int* __restrict__ done) {
+    if (*done) return;
+    sc[SC_RHO_OLD] = sc[SC_RHO];
+}
+
+// BiCGStab (right Jacobi preconditioning), van der Vorst's iteration:
+// p = r + beta (p - omega v), beta = (rho / rho_old)(alpha / omega)
+__global__ void bicgstab_dir_kernel(double* __restrict__ sc, const double* __restrict__ r,
+                                    const double* __restrict__ v, int64_t n, int first, double* __restrict__ p,
+                                    int* __restrict__ done, int* __restrict__ info) {
+    if (*done) return;
+    const double rho = sc[SC_RHO];
+    if (rho == 0.0 || !isfinite(rho) || (!first && sc[SC_OMEGA] == 0.0)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double beta = first ? 0.0 : (rho / sc[SC_RHO_OLD]) * (sc[SC_ALPHA] / sc[SC_OMEGA]);
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p[i] = first ? r[i] : r[i] + beta * (p[i] - sc[SC_OMEGA] * v[i]);
+}
+
+// alpha = rho / (r0 . v); s = r - alpha v
+__global__ void bicgstab_s_kernel(double* __restrict__ sc, const double* __restrict__ r,
+                                  const double* __restrict__ v, int64_t n, double* __restrict__ s,
+                                  int* __restrict__ done, int* __restrict__ info) {
+    if (*done) return;
+    const double den = sc[SC_DEN];
+    if (den == 0.0 || !isfinite(den)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double alpha = sc[SC_RHO] / den;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) sc[SC_ALPHA] = alpha;
+    if (i >= n) return;
+    s[i] = r[i] - alpha * v[i];
+}
+
+// omega = (t . s) / (t . t); x += alpha p^ + omega s^; r = s - omega t
+__global__ void bicgstab_x_kernel(double* __restrict__ sc, const double* __restrict__ ph,
+                                  const double* __restrict__ sh, const double* __restrict__ s,
+                                  const double* __restrict__ t, int64_t n, double* __restrict__ x,
+                                  double* __restrict__ r, const int* __restrict__ done) {
+    if (*done) return;
+    const double tt = sc[SC_TT];
+    const double omega = tt != 0.0 ? sc[SC_TS] / tt : 0.0;
+    const double alpha = sc[SC_ALPHA];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) sc[SC_OMEGA] = omega;
+    if (i >= n) return;
+    x[i] += alpha * ph[i] + omega * sh[i];
+    r[i] = s[i] - omega * t[i];
+}
+
+// y = a (copy)
+__global__ void copy_kernel(const double* __restrict__ a, int64_t n, double* __restrict__ y) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = a[i];
+}
+
+// y = a .* dinv
+__global__ void scale_kernel(const double* __restrict__ a, const double* __restrict__ dinv, int64_t n,
+                             double* __restrict__ y, const int* __restrict__ done) {
+    if (done && *done) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = a[i] * dinv[i];
+}
+
+// dinv[i] = 1 / K_ii (zero diagonal -> 1, the row is then left unpreconditioned)
+__global__ void jacobi_setup_kernel(const double* __restrict__ vals, const int64_t* __restrict__ diag_pos, int64_t n,
+                                    double* __restrict__ dinv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = vals[diag_pos[i]];
+    dinv[i] = d != 0.0 ? 1.0 / d : 1.0;
+}
+
+// u += du
+__global__ void add_kernel(const double* __restrict__ du, int64_t n, double* __restrict__ u) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) u[i] += du[i];
+}
+
+}  // namespace cp

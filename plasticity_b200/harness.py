@@ -169,8 +169,15 @@ class NewtonHarness:
     """Fixed-iteration Newton loop over a structured Q1 mesh."""
 
     def __init__(self, backend, mesh: StructuredMesh, bc_table, n_increments: int, max_newton: int = 4,
-                 multiphase: bool = False):
+                 multiphase: bool = False, device_system: bool = False, solver=None):
+        """device_system: run the global system on the GPU (cp_bind_dofs /
+        cp_newton_iteration / cp_update_from_displacement) with 'solver'
+        (capi.CpSolver, default BiCG 1e-10); otherwise assemble on the
+        backend and solve on the host with a sparse LU."""
         self.be = backend
+        self.device_system = device_system
+        self.solver = solver
+        self.solve_info = []
         self.mesh = mesh
         self.n_increments = n_increments
         self.max_newton = max_newton
@@ -186,6 +193,8 @@ class NewtonHarness:
         self._zero_entries = mask[mesh._rows] | mask[mesh._indices]
         self._diag = None
         backend.bind_mesh(mesh.n_cells, mesh.grad_N, mesh.JxW, True)
+        if device_system:
+            backend.bind_dofs(mesh.n_dofs, mesh.cell_dofs, self.cdofs)
 
     def _solve(self, K, R, duc):
         """K du = R with du[c] = duc (constraints condensed as deal.II's
@@ -202,14 +211,21 @@ class NewtonHarness:
     def step(self):
         """One increment: max_newton assemble+solve passes, then the commit."""
         mesh = self.mesh
-        for it in range(self.max_newton):
-            Ke, Re, st = self.be.assemble(self.u[mesh.cell_dofs], self.F_e, self.F_r)
-            K = mesh.assemble_matrix(Ke)
-            R = mesh.assemble_vector(Re)
-            duc = self.cvals if it == 0 else np.zeros_like(self.cvals)
-            self.u += self._solve(K, R, duc)
-        F = mesh.deformation_gradients(self.u)
-        self.be.update(F, 0, self.F_e, self.F_r)
+        if self.device_system:
+            for it in range(self.max_newton):
+                self.solve_info.append(self.be.newton_iteration(self.cvals if it == 0 else None, self.F_e, self.F_r,
+                                                                self.solver))
+            self.be.update_from_displacement(self.F_e, self.F_r)
+            self.u = self.be.get_displacement()
+        else:
+            for it in range(self.max_newton):
+                Ke, Re, st = self.be.assemble(self.u[mesh.cell_dofs], self.F_e, self.F_r)
+                K = mesh.assemble_matrix(Ke)
+                R = mesh.assemble_vector(Re)
+                duc = self.cvals if it == 0 else np.zeros_like(self.cvals)
+                self.u += self._solve(K, R, duc)
+            F = mesh.deformation_gradients(self.u)
+            self.be.update(F, 0, self.F_e, self.F_r)
         avg = self.be.averages()
         self.be.reorient()
         self.be.commit()
@@ -233,8 +249,9 @@ class NewtonHarness:
         return np.array(self.rows)
 
 
-def kat_setup(fixture, backend_factory, material_from_fixture):
-    """Build mesh/backend/harness for a tests/golden/kat_*.npz fixture."""
+def kat_setup(fixture, backend_factory, material_from_fixture, **harness_kw):
+    """Build mesh/backend/harness for a tests/golden/kat_*.npz fixture
+    (harness_kw: NewtonHarness options such as device_system, solver)."""
     d = dict(np.load(fixture))
     mesh = StructuredMesh(tuple(int(x) for x in d["n_elem"]))
     mat = material_from_fixture(d)
@@ -242,5 +259,5 @@ def kat_setup(fixture, backend_factory, material_from_fixture):
     be = backend_factory([mat], d)
     rod = np.repeat(d["cell_rodrigues"], 8, axis=0)
     be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
-    h = NewtonHarness(be, mesh, d["bc"], n_inc, int(d["max_newton"]))
+    h = NewtonHarness(be, mesh, d["bc"], n_inc, int(d["max_newton"]), **harness_kw)
     return h, d
