@@ -42,29 +42,77 @@ def test_device_newton_matches_host_direct_solve(cuda_lib, kind):
     hd.be.close()
 
 
-def test_device_newton_mixed_lattices_and_precond_norm(cuda_lib):
-    """A 4x4x4 mesh whose cells alternate FCC and HCP grains under the deck's
-    tension BCs; the device loop with PETSc's preconditioned-residual test
-    against the host direct solve."""
+def _mixed_runs(variants, n_inc=4):
     mesh = H.StructuredMesh((4, 4, 4))
     rng = np.random.default_rng(23)
     cl = (np.arange(mesh.n_cells) % 2).astype(np.int32)
     rod = np.repeat(M.random_rodrigues(rng, mesh.n_cells), 8, axis=0)
     # faces 1/3/5 (x=0, y=0, z=0) held in x/y/z, face 2 (x=1) pulled to u_x = 0.004 over 8 increments
     bc = np.array([[1, 1, 0.0], [3, 2, 0.0], [5, 3, 0.0], [2, 1, 0.004]])
-    runs = []
-    for dev in (False, True):
+    out = []
+    for dev, solver in variants:
         be = CpHandle([M.fcc_cu(), M.hcp_mg()])
         be.bind_qps(np.repeat(cl, 8), rod)
-        h = H.NewtonHarness(be, mesh, bc, 8, 4, device_system=dev,
-                            solver=default_solver(precond_norm=1) if dev else None)
-        runs.append((h, h.run(4)))
-    (hh, rh), (hd, rd) = runs
+        h = H.NewtonHarness(be, mesh, bc, 8, 4, device_system=dev, solver=solver)
+        rows = h.run(n_inc)
+        h.stats = be.stats()
+        out.append((h, rows))
+        be.close()
+    return out
+
+
+def test_device_newton_mixed_lattices(cuda_lib):
+    """Cells alternating FCC and HCP grains under tension BCs: the device loop
+    against the host direct solve.  The first increment agrees to the solver
+    tolerance.  Later increments create active-set solves with condition up to
+    1e17 (flagged per qp), whose results are set by rounding: perturbing each
+    Newton update of the oracle's own loop by 1e-12 moves its final stresses by
+    ~1 %, so only a loose bound holds there."""
+    (hh, rh), (hd, rd) = _mixed_runs([(False, None), (True, default_solver())])
     assert all(i["converged"] for i in hd.solve_info)
     assert np.abs(rh[:, 6:12]).max() > 20.0  # MPa: past the 5-16 MPa critical resolved shear stresses
-    assert rel_err(rd[:, :12], rh[:, :12]) < 1e-4
-    hh.be.close()
-    hd.be.close()
+    assert rel_err(rd[:1, :12], rh[:1, :12]) < 1e-6
+    assert (hh.stats[:, 7] > 12).any() and (hd.stats[:, 7] > 12).any()
+    assert np.abs(rd[:, 6:9] - rh[:, 6:9]).max() < 3e-2 * np.abs(rh[:, 6:9]).max()
+
+
+def test_device_newton_iteration_solves_the_condensed_system(cuda_lib):
+    """From one state, a device Newton iteration and the host's condensed
+    direct solve of the same assembled system give the same du."""
+    mesh = H.StructuredMesh((4, 4, 4))
+    rng = np.random.default_rng(29)
+    rod = np.repeat(M.random_rodrigues(rng, mesh.n_cells), 8, axis=0)
+    bc = np.array([[1, 1, 0.0], [3, 2, 0.0], [5, 3, 0.0], [2, 1, 0.004]])
+    be = CpHandle([M.fcc_cu()])
+    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+    h = H.NewtonHarness(be, mesh, bc, 8, 4, device_system=True)
+    h.run(2)
+    u0 = be.get_displacement()
+    for kind in (CP_SOLVER_BICG, CP_SOLVER_BICGSTAB):
+        be.set_displacement(u0)
+        Ke, Re, _ = be.assemble(u0[mesh.cell_dofs], h.F_e, h.F_r)
+        K, R = mesh.assemble_matrix(Ke), mesh.assemble_vector(Re)
+        du_ref = h._solve(K, R, h.cvals)
+        info = be.newton_iteration(h.cvals, h.F_e, h.F_r, default_solver(kind=kind))
+        du = be.get_displacement() - u0
+        assert info["converged"] and info["iterations"] > 0
+        assert np.abs(du - du_ref).max() <= 1e-7 * np.abs(du_ref).max(), kind
+        assert np.allclose(du[h.cdofs], h.cvals, rtol=1e-12, atol=1e-15)  # prescribed increments distributed
+    be.close()
+
+
+def test_device_newton_petsc_norm(cuda_lib):
+    """The stopping test PETSc's BiCG applies (preconditioned residual
+    ||M^-1 r|| <= 1e-10 ||b||).  With Jacobi, M^-1 scales the residual by the
+    inverse diagonal (~1e-5 here), so it stops far earlier than the true
+    residual test: fewer iterations and ~1e-3 in the stresses, which is the
+    accuracy of the reference's own linear solves."""
+    (ht, rt), (hp, rp) = _mixed_runs([(True, default_solver()), (True, default_solver(precond_norm=1))])
+    assert all(i["converged"] for i in hp.solve_info)
+    it_t = sum(i["iterations"] for i in ht.solve_info)
+    it_p = sum(i["iterations"] for i in hp.solve_info)
+    assert it_p < it_t, (it_p, it_t)
+    assert np.abs(rp[:, 6:9] - rt[:, 6:9]).max() < 1e-2 * np.abs(rt[:, 6:9]).max()
 
 
 def test_device_system_errors(cuda_lib):
