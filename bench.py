@@ -360,6 +360,7 @@ def ours(args):
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, parity = cpu_leg(args, h, Fn, P, dPdF, lid, rod)
+    rve = rve_leg(args, local) if (world == 1 and not args.no_rve) else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "qp-updates/s", "n_gpus": world, "steps": args.steps,
@@ -386,6 +387,7 @@ def ours(args):
         "qp_error_flags": bad,
         "cpu_baseline": cpu,
         "parity": parity,
+        "rve": rve,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -434,6 +436,76 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
     return cpu, parity
 
 
+# --------------------------------------------------------------------- RVE solve
+RVE_INC, RVE_NEWTON = 20, 4
+
+
+def rve_case():
+    """The 8x8x8 FCC Cu cube: one grain per element (Rodrigues of a normalised
+    N(0, I4) quaternion, seed SEED_ORIENT), faces x=0 held in x/y/z, face x=1
+    pulled to u_x = 0.02 in 20 equal increments, 4 Newton iterations each."""
+    from plasticity_b200 import harness as H
+    from plasticity_b200 import materials as M
+    mesh = H.StructuredMesh((8, 8, 8))
+    rod = np.repeat(M.random_rodrigues(np.random.default_rng(SEED_ORIENT), mesh.n_cells), 8, axis=0)
+    bc = np.array([[1, 1, 0.0], [1, 2, 0.0], [1, 3, 0.0], [2, 1, 0.02]])
+    return mesh, rod, bc
+
+
+def rve_run(backend, device_system):
+    from plasticity_b200 import harness as H
+    mesh, rod, bc = rve_case()
+    backend.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+    h = H.NewtonHarness(backend, mesh, bc, RVE_INC, RVE_NEWTON, device_system=device_system)
+    t0 = time.perf_counter()
+    rows = h.run()
+    return rows, time.perf_counter() - t0, h
+
+
+def rve_leg(args, device):
+    """RVE solves/s on the 4,096-qp FCC cube: the whole Newton loop on the
+    device (sorted update, device scatter, condensation and BiCG) against the
+    plain FP64 GPU drop-in (plain update kernel, host direct solve), whose
+    stress-strain rows set the stress error, and the oracle with the host
+    solve on the host cores."""
+    from plasticity_b200 import materials as M
+    from plasticity_b200.capi import CpHandle, default_options
+    mats = [M.fcc_cu()]
+    hw = CpHandle(mats, default_options(device=device))
+    rve_run(hw, True)  # warm-up: first launches, allocations
+    hw.close()
+    hd = CpHandle(mats, default_options(device=device))
+    rows_d, t_d, harness = rve_run(hd, True)
+    iters = [i["iterations"] for i in harness.solve_info]
+    hd.close()
+    hp = CpHandle(mats, default_options(device=device, plain_kernel=1))
+    rows_p, t_p, _ = rve_run(hp, False)
+    hp.close()
+    hs = CpHandle(mats, default_options(device=device))
+    rows_s, t_s, _ = rve_run(hs, False)
+    ill = int((hs.stats()[:, 7] > 12).sum())
+    hs.close()
+    serr = lambda r: float(np.abs(r[:, 6:12] - rows_p[:, 6:12]).max() / np.abs(rows_p[:, 6:12]).max())
+    err = serr(rows_d)
+    out = {"workload": "8x8x8 Q1 FCC Cu cube, 512 grains, x-tension to 2% in 20 increments x (4 Newton + post-pass)",
+           "qp_updates": RVE_INC * (RVE_NEWTON + 1) * 4096,
+           "rve_solves_per_s": 1.0 / t_d, "seconds": t_d, "linear_iterations_mean": float(np.mean(iters)),
+           "stress_rel_err_vs_plain_gpu": err,
+           "plain_gpu_host_solve": {"seconds": t_p, "rve_solves_per_s": 1.0 / t_p},
+           "sorted_update_host_solve": {"seconds": t_s, "stress_rel_err_vs_plain_gpu": serr(rows_s)},
+           "ill_conditioned_qps_at_end": ill,
+           "final_stress_xx_mpa": float(rows_d[-1, 6])}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        ob = O.OracleBackend(mats, default_options(), nthreads=threads)
+        rows_c, t_c, _ = rve_run(ob, False)
+        out["cpu_baseline"] = {"seconds": t_c, "rve_solves_per_s": 1.0 / t_c, "cores": threads, "kind": "port",
+                               "stress_rel_err_vs_plain_gpu": float(np.abs(rows_c[:, 6:12] - rows_p[:, 6:12]).max()
+                                                                    / np.abs(rows_p[:, 6:12]).max())}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -445,6 +517,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain thread-per-qp kernel")
+    ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
