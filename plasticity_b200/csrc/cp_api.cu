@@ -323,7 +323,14 @@ struct cp_handle {
         double *d_vals = nullptr, *d_Ke = nullptr, *d_Re = nullptr, *d_Ul = nullptr, *d_duc = nullptr;
         double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
         double *d_sc = nullptr, *d_partial = nullptr;
+        double* d_fpartial = nullptr;           // per-block partials of the fused iteration (n_dofs / 8 + 64)
+        unsigned int* d_ticket = nullptr;       // arrival counters of the fused reductions (4)
         int *d_done = nullptr, *d_info = nullptr;
+        // a block of Krylov iterations captured as CUDA graphs (first block /
+        // later blocks), for the solver settings they were captured with
+        cudaGraphExec_t g_first = nullptr, g_next = nullptr;
+        int g_kind = -1, g_precond = -1, g_every = 0;
+        double g_tol = -1.0;
     } sys;
     // averages scratch
     double *d_avg_partial = nullptr, *d_avg_out = nullptr;
@@ -428,8 +435,12 @@ void free_system(cp_handle* h) {
     cudaFree(y.d_vec);
     cudaFree(y.d_sc);
     cudaFree(y.d_partial);
+    cudaFree(y.d_fpartial);
+    cudaFree(y.d_ticket);
     cudaFree(y.d_done);
     cudaFree(y.d_info);
+    if (y.g_first) cudaGraphExecDestroy(y.g_first);
+    if (y.g_next) cudaGraphExecDestroy(y.g_next);
     y = cp_handle::System{};
 }
 
@@ -1337,6 +1348,8 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
               cudaMalloc(&y.d_vec, sizeof(double) * SYS_VECS * n_dofs) == cudaSuccess &&
               cudaMalloc(&y.d_sc, sizeof(double) * SC_COUNT) == cudaSuccess &&
               cudaMalloc(&y.d_partial, sizeof(double) * RED_BLOCKS) == cudaSuccess &&
+              cudaMalloc(&y.d_fpartial, sizeof(double) * (n_dofs / 8 + 64)) == cudaSuccess &&
+              cudaMalloc(&y.d_ticket, sizeof(unsigned int) * 4) == cudaSuccess &&
               cudaMalloc(&y.d_done, sizeof(int)) == cudaSuccess && cudaMalloc(&y.d_info, sizeof(int) * 3) == cudaSuccess;
     if (!ok) {
         free_system(h);
@@ -1355,6 +1368,7 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
         CK(h, cudaMemcpy(y.d_con, h_constrained, sizeof(int64_t) * n_constrained, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(y.d_cmask, cmask.data(), n_dofs, cudaMemcpyHostToDevice));
     CK(h, cudaMemset(y.d_vec, 0, sizeof(double) * SYS_VECS * n_dofs));
+    CK(h, cudaMemset(y.d_ticket, 0, sizeof(unsigned int) * 4));
     return CP_OK;
 }
 
@@ -1418,15 +1432,19 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
         bicgstab_x_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_PH), v(V_SH), v(V_S), v(V_T), n, v(V_X),
                                                                v(V_RES), done);
     } else {
-        jacobi2_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_DINV), v(V_RES), v(V_RT), n, v(V_Z), v(V_ZT), done);
-        sys_dot(h, v(V_Z), v(V_RT), SC_RHO, done);
-        bicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
-                                                             s.d_done, s.d_info);
-        sys_spmv(h, v(V_P), v(V_Q), false, done);
-        sys_spmv(h, v(V_PT), v(V_QT), true, done);
-        sys_dot(h, v(V_PT), v(V_Q), SC_DEN, done);
-        bicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_P), v(V_Q), v(V_QT), n, v(V_X), v(V_RES),
-                                                              v(V_RT), s.d_done, s.d_info);
+        // BiCG in four kernels; the last one also tests convergence
+        fbicg_precond_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_DINV), v(V_RES), v(V_RT), n, v(V_Z), v(V_ZT),
+                                                                  s.d_sc, s.d_fpartial, s.d_ticket + 0, done);
+        fbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
+                                                              s.d_done, s.d_info);
+        fbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+            s.d_row_ptr, s.d_col, s.d_vals, s.d_tpos, v(V_P), v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
+            s.d_ticket + 1, done);
+        fbicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_P), v(V_Q), v(V_QT), v(V_DINV), n,
+                                                               sv.rel_tolerance, sv.precond_norm, v(V_X), v(V_RES),
+                                                               v(V_RT), s.d_fpartial, s.d_ticket + 2, s.d_done,
+                                                               s.d_info);
+        return;
     }
     sys_dot(h, v(V_RES), v(V_RES), SC_RR, done);
     if (sv.precond_norm) {
@@ -1435,6 +1453,38 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
     }
     check_kernel<<<1, 1, 0, h->stream>>>(s.d_sc, sv.rel_tolerance, sv.precond_norm, s.d_done, s.d_info);
     shift_rho_kernel<<<1, 1, 0, h->stream>>>(s.d_sc, done);
+}
+
+// Capture 'every' Krylov iterations as two graphs (the first block, whose
+// first iteration starts the recurrences, and later blocks).  Returns false
+// (plain launches are used) if capture is not possible.
+bool ensure_solve_graphs(cp_handle* h, const cp_solver_t& sv, int every) {
+    auto& s = h->sys;
+    if (s.g_first && s.g_next && s.g_kind == sv.kind && s.g_precond == sv.precond_norm && s.g_every == every &&
+        s.g_tol == sv.rel_tolerance)
+        return true;
+    if (s.g_first) cudaGraphExecDestroy(s.g_first);
+    if (s.g_next) cudaGraphExecDestroy(s.g_next);
+    s.g_first = s.g_next = nullptr;
+    for (int f = 1; f >= 0; --f) {
+        if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+        for (int t = 0; t < every; ++t) krylov_iteration(h, sv, f == 1 && t == 0);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        cudaGraphExec_t ex = nullptr;
+        const bool ok = e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            cudaGetLastError();
+            return false;
+        }
+        (f ? s.g_first : s.g_next) = ex;
+    }
+    s.g_kind = sv.kind;
+    s.g_precond = sv.precond_norm;
+    s.g_every = every;
+    s.g_tol = sv.rel_tolerance;
+    return true;
 }
 
 }  // namespace
@@ -1496,6 +1546,7 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     CK(h, cudaMemsetAsync(s.d_done, 0, sizeof(int), h->stream));
     CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
     CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
+    CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 4, h->stream));
     sys_dot(h, v(V_RHS), v(V_RHS), SC_BB, nullptr);
     sys_dot(h, v(V_RHS), v(V_RHS), SC_RR, nullptr);
     if (sv.precond_norm) {
@@ -1511,10 +1562,14 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         hinfo[1] = 1;  // du = 0 solves it
     } else {
         const int every = sv.check_every > 0 ? sv.check_every : 8;
+        const bool graphs = ensure_solve_graphs(h, sv, every);
         int queued = 0;
         while (queued < sv.max_iterations) {
             const int k = std::min(every, sv.max_iterations - queued);
-            for (int t = 0; t < k; ++t) krylov_iteration(h, sv, queued + t == 0);
+            if (graphs && k == every)
+                CK(h, cudaGraphLaunch(queued == 0 ? s.g_first : s.g_next, h->stream));
+            else
+                for (int t = 0; t < k; ++t) krylov_iteration(h, sv, queued + t == 0);
             queued += k;
             CK(h, cudaGetLastError());
             CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof hinfo, cudaMemcpyDeviceToHost, h->stream));

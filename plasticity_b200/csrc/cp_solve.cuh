@@ -161,59 +161,6 @@ __global__ void check_kernel(double* __restrict__ sc, double tol, int precond_no
     }
 }
 
-// z = r / d, z~ = r~ / d  (Jacobi: M = diag K)
-__global__ void jacobi2_kernel(const double* __restrict__ dinv, const double* __restrict__ r,
-                               const double* __restrict__ rt, int64_t n, double* __restrict__ z,
-                               double* __restrict__ zt, const int* __restrict__ done) {
-    if (*done) return;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    z[i] = r[i] * dinv[i];
-    if (zt) zt[i] = rt[i] * dinv[i];
-}
-
-// BiCG direction update: p = z + beta p, p~ = z~ + beta p~ (beta = rho / rho_old; first: beta = 0)
-__global__ void bicg_dir_kernel(double* __restrict__ sc, const double* __restrict__ z,
-                                const double* __restrict__ zt, int64_t n, int first, double* __restrict__ p,
-                                double* __restrict__ pt, int* __restrict__ done, int* __restrict__ info) {
-    if (*done) return;
-    const double rho = sc[SC_RHO];
-    if (rho == 0.0 || !isfinite(rho)) {  // breakdown: stop (thread-uniform decision)
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            info[2] = 1;
-            *done = 1;
-        }
-        return;
-    }
-    const double beta = first ? 0.0 : rho / sc[SC_RHO_OLD];
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    p[i] = z[i] + beta * p[i];
-    pt[i] = zt[i] + beta * pt[i];
-}
-
-// x += alpha p; r -= alpha q; r~ -= alpha q~  (alpha = rho / (p~ . q))
-__global__ void bicg_step_kernel(double* __restrict__ sc, const double* __restrict__ p, const double* __restrict__ q,
-                                 const double* __restrict__ qt, int64_t n, double* __restrict__ x,
-                                 double* __restrict__ r, double* __restrict__ rt, int* __restrict__ done,
-                                 int* __restrict__ info) {
-    if (*done) return;
-    const double den = sc[SC_DEN];
-    if (den == 0.0 || !isfinite(den)) {  // breakdown (thread-uniform decision)
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            info[2] = 1;
-            *done = 1;
-        }
-        return;
-    }
-    const double alpha = sc[SC_RHO] / den;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    x[i] += alpha * p[i];
-    r[i] -= alpha * q[i];
-    rt[i] -= alpha * qt[i];
-}
-
 // scalar bookkeeping between iterations: rho_old = rho
 __global__ void shift_rho_kernel(double* __restrict__ sc, const int* __restrict__ done) {
     if (*done) return;
@@ -303,6 +250,144 @@ __global__ void jacobi_setup_kernel(const double* __restrict__ vals, const int64
 __global__ void add_kernel(const double* __restrict__ du, int64_t n, double* __restrict__ u) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) u[i] += du[i];
+}
+
+// ---- fused BiCG iteration: 4 kernels, each reduction finished by the last
+// block to arrive (its partial written, __threadfence, an atomic ticket; the
+// last block sums the partials in block order, so the result is
+// deterministic; nothing waits on another block)
+
+// the block's partial of v into partial[blockIdx.x]; true in every thread of
+// the block that finished last, which then holds sum(partial) in order in *out
+__device__ __forceinline__ bool last_block_sum(double v, double* __restrict__ partial,
+                                               unsigned int* __restrict__ ticket, double* __restrict__ out) {
+    __shared__ bool is_last;
+    const double s = block_sum(v);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = s;
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double f = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) f += ((volatile double*)partial)[b];
+    f = block_sum(f);
+    if (threadIdx.x == 0) {
+        *out = f;
+        *ticket = 0u;
+    }
+    return true;
+}
+
+// (1) z = r / d, z~ = r~ / d; rho = z . r~
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_precond_kernel(
+    const double* __restrict__ dinv, const double* __restrict__ r, const double* __restrict__ rt, int64_t n,
+    double* __restrict__ z, double* __restrict__ zt, double* __restrict__ sc, double* __restrict__ partial,
+    unsigned int* __restrict__ ticket, const int* __restrict__ done) {
+    if (*done) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < n) {
+        const double a = r[i] * dinv[i], b = rt[i] * dinv[i];
+        z[i] = a;
+        zt[i] = b;
+        v = a * rt[i];
+    }
+    last_block_sum(v, partial, ticket, sc + SC_RHO);
+}
+
+// (2) p = z + beta p, p~ = z~ + beta p~ (beta = rho / rho_old, 0 on the first
+// iteration); breakdown when rho is zero
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_dir_kernel(
+    const double* __restrict__ sc, const double* __restrict__ z, const double* __restrict__ zt, int64_t n, int first,
+    double* __restrict__ p, double* __restrict__ pt, int* __restrict__ done, int* __restrict__ info) {
+    if (*done) return;
+    const double rho = sc[SC_RHO];
+    if (rho == 0.0 || !isfinite(rho)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double beta = first ? 0.0 : rho / sc[SC_RHO_OLD];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p[i] = z[i] + beta * p[i];
+    pt[i] = zt[i] + beta * pt[i];
+}
+
+// (3) q = K p and q~ = K^T p~ (a warp per row, both in one pass over the
+// row); den = p~ . q
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv_kernel(
+    const int64_t* __restrict__ row_ptr, const int* __restrict__ col, const double* __restrict__ vals,
+    const int64_t* __restrict__ tpos, const double* __restrict__ p, const double* __restrict__ pt, int64_t n,
+    double* __restrict__ q, double* __restrict__ qt, double* __restrict__ sc, double* __restrict__ partial,
+    unsigned int* __restrict__ ticket, const int* __restrict__ done) {
+    if (*done) return;
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    double v = 0.0;
+    if (row < n) {
+        double s = 0.0, st = 0.0;
+        for (int64_t k = row_ptr[row] + lane; k < row_ptr[row + 1]; k += 32) {
+            const int c = col[k];
+            s += vals[k] * p[c];
+            st += vals[tpos[k]] * pt[c];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+            st += __shfl_xor_sync(0xffffffffu, st, o);
+        }
+        if (lane == 0) {
+            q[row] = s;
+            qt[row] = st;
+            v = pt[row] * s;
+        }
+    }
+    last_block_sum(v, partial, ticket, sc + SC_DEN);
+}
+
+// (4) x += alpha p; r -= alpha q; r~ -= alpha q~ (alpha = rho / den);
+// ||r||^2 (and ||M^-1 r||^2), then the convergence test in the last block;
+// rho_old = rho for the next iteration
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_step_kernel(
+    double* __restrict__ sc, const double* __restrict__ p, const double* __restrict__ q, const double* __restrict__ qt,
+    const double* __restrict__ dinv, int64_t n, double tol, int precond_norm, double* __restrict__ x,
+    double* __restrict__ r, double* __restrict__ rt, double* __restrict__ partial, unsigned int* __restrict__ ticket,
+    int* __restrict__ done, int* __restrict__ info) {
+    if (*done) return;
+    const double den = sc[SC_DEN];
+    if (den == 0.0 || !isfinite(den)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            info[2] = 1;
+            *done = 1;
+        }
+        return;
+    }
+    const double alpha = sc[SC_RHO] / den;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < n) {
+        x[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        rt[i] -= alpha * qt[i];
+        v = precond_norm ? (ri * dinv[i]) * (ri * dinv[i]) : ri * ri;
+    }
+    if (last_block_sum(v, partial, ticket, sc + (precond_norm ? SC_ZZ : SC_RR)) && threadIdx.x == 0) {
+        info[0] += 1;
+        const double rn = sqrt(sc[precond_norm ? SC_ZZ : SC_RR]);
+        if (rn <= tol * sqrt(sc[SC_BB])) {
+            info[1] = 1;
+            *done = 1;
+        }
+        sc[SC_RHO_OLD] = sc[SC_RHO];
+    }
 }
 
 }  // namespace cp
