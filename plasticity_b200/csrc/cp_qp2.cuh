@@ -75,6 +75,43 @@ __host__ __device__ __forceinline__ void row_axpy(double* ai, const double* aj, 
     }
     for (; c < m; ++c) ai[c] -= f * aj[c];
 }
+// The same on four rows i0..i0+3 at once (row stride ld): the pivot row's
+// columns are loaded once per step and all 16 row entries before any store.
+__host__ __device__ __forceinline__ void rows4_axpy(double* a, int ld, const double* aj, const double f[4], int c0,
+                                                   int m) {
+    double* a0 = a;
+    double* a1 = a + ld;
+    double* a2 = a + 2 * ld;
+    double* a3 = a + 3 * ld;
+    int c = c0;
+    for (; c + 4 <= m; c += 4) {
+        double x[4], y0[4], y1[4], y2[4], y3[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            x[u] = aj[c + u];
+            y0[u] = a0[c + u];
+            y1[u] = a1[c + u];
+            y2[u] = a2[c + u];
+            y3[u] = a3[c + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0[c + u] = y0[u] - f[0] * x[u];
+            a1[c + u] = y1[u] - f[1] * x[u];
+            a2[c + u] = y2[u] - f[2] * x[u];
+            a3[c + u] = y3[u] - f[3] * x[u];
+        }
+    }
+    for (; c < m; ++c) {
+        const double x = aj[c];
+        const double y0 = a0[c], y1 = a1[c], y2 = a2[c], y3 = a3[c];
+        a0[c] = y0 - f[0] * x;
+        a1[c] = y1 - f[1] * x;
+        a2[c] = y2 - f[2] * x;
+        a3[c] = y3 - f[3] * x;
+    }
+}
+
 __host__ __device__ __forceinline__ void row_swap(double* a, double* b, int m) {
     int c = 0;
     for (; c + 4 <= m; c += 4) {
@@ -126,7 +163,20 @@ __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, dou
         double bj[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) bj[c] = B[j * NRHS + c];
-        for (int i = j + 1; i < m; ++i) {
+        int i = j + 1;
+        // four rows per pass (a zero multiplier leaves its row's finite
+        // entries unchanged, as skipping it would)
+        for (; i + 4 <= m; i += 4) {
+            double f[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) f[r] = A[(i + r) * ld + j] * piv;
+            rows4_axpy(A + i * ld, ld, A + j * ld, f, j + 1, m);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) B[(i + r) * NRHS + c] -= f[r] * bj[c];
+        }
+        for (; i < m; ++i) {
             const double f = A[i * ld + j] * piv;
             if (f == 0.0) continue;
             row_axpy(A + i * ld, A + j * ld, f, j + 1, m);
@@ -392,7 +442,18 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 for (int r = 0; r < m; ++r) {
                     const int kr = w.pos[r];
                     w.rhs[r] = w.b[kr];
-                    for (int c = 0; c < m; ++c) w.Apa[r * PMAX + c] = w.A[kr * p_init + w.pos[c]];
+                    const double* Ar = w.A + kr * p_init;
+                    double* Pr = w.Apa + r * PMAX;
+                    int c = 0;
+                    for (; c + 4 <= m; c += 4) {  // four gathers in flight per step
+                        const int c0 = w.pos[c], c1 = w.pos[c + 1], c2 = w.pos[c + 2], c3 = w.pos[c + 3];
+                        const double v0 = Ar[c0], v1 = Ar[c1], v2 = Ar[c2], v3 = Ar[c3];
+                        Pr[c] = v0;
+                        Pr[c + 1] = v1;
+                        Pr[c + 2] = v2;
+                        Pr[c + 3] = v3;
+                    }
+                    for (; c < m; ++c) Pr[c] = Ar[w.pos[c]];
                 }
                 double cnd = 1.0;
                 if (lu_solve_b<1>(w.Apa, m, PMAX, w.rhs, &cnd)) status |= QP_SINGULAR;
