@@ -85,6 +85,24 @@ def bytes_per_qp(n, ns, nw, flag):
     return rd + wr
 
 
+# --------------------------------------------------------------------- replicas
+def max_over_ranks(x: float, device) -> float:
+    """The largest x over all ranks (a no-op without a process group): the
+    job's time is its slowest replica's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(world: int, n_qp_per_rank: int, steps: int, seconds: float) -> float:
+    """Whole-job qp-updates/s: every rank's qps over the slowest rank's time."""
+    return world * n_qp_per_rank * steps / seconds
+
+
 # --------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples during the timed region (read-only queries)."""
@@ -264,12 +282,9 @@ def ours(args):
     elapsed_ms = e0.elapsed_time(e1)
     timing = h.get_timing()
     h.set_timing(False)
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dev)
     ms_per_step = elapsed_ms / args.steps
-    value = world * n * args.steps / (elapsed_ms * 1e-3)
+    value = aggregate_value(world, n, args.steps, elapsed_ms * 1e-3)
 
     # the plain thread-per-qp drop-in (cp_options_t.plain_kernel) on the same
     # inputs and history, for the speed-up of the optimised pipeline over it
@@ -346,12 +361,8 @@ def ours(args):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             assert call() == 0
-        dt = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([dt], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
-        e2e = {"value": world * n * args.steps / dt, "unit": "qp-updates/s",
+        dt = max_over_ranks(time.perf_counter() - t0, dev)
+        e2e = {"value": aggregate_value(world, n, args.steps, dt), "unit": "qp-updates/s",
                "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": (9 + 81) * 8 * n + 4 * n,
                "ms_per_step": 1e3 * dt / args.steps}
 
