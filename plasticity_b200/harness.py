@@ -249,10 +249,10 @@ class NewtonHarness:
         return np.array(self.rows)
 
 
-def kat_setup(fixture, backend_factory, material_from_fixture, **harness_kw):
-    """Build mesh/backend/harness for a tests/golden/kat_*.npz fixture
-    (harness_kw: NewtonHarness options such as device_system, solver)."""
-    d = dict(np.load(fixture))
+def deck_setup(d, backend_factory, material_from_fixture, **harness_kw):
+    """Build mesh/backend/harness from a parsed deck (decks.load_deck, or a
+    tests/golden/kat_*.npz fixture's dict); harness_kw: NewtonHarness options
+    such as device_system, solver."""
     mesh = StructuredMesh(tuple(int(x) for x in d["n_elem"]))
     mat = material_from_fixture(d)
     n_inc = int(round(float(d["total_T"]) / float(d["delT"])))
@@ -261,3 +261,8 @@ def kat_setup(fixture, backend_factory, material_from_fixture, **harness_kw):
     be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
     h = NewtonHarness(be, mesh, d["bc"], n_inc, int(d["max_newton"]), **harness_kw)
     return h, d
+
+
+def kat_setup(fixture, backend_factory, material_from_fixture, **harness_kw):
+    """deck_setup for a tests/golden/kat_*.npz fixture."""
+    return deck_setup(dict(np.load(fixture)), backend_factory, material_from_fixture, **harness_kw)
