@@ -531,7 +531,7 @@ void sort_group(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m) {
 template <int PMAX, class FSrc>
 void launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m, int flag, double F_e, double F_r,
                     double* P, double* T, double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
-    update2_kernel<PMAX, FSrc><<<blocks_for(m, UPDATE2_BLOCK), UPDATE2_BLOCK, 0, h->stream>>>(
+    update2_kernel<PMAX, FSrc><<<blocks_for(m, update2_block(PMAX)), update2_block(PMAX), 0, h->stream>>>(
         h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats,
         kF, kT, g.lattice);
 }

@@ -232,13 +232,23 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
 // similar size.  (Interleaving large- and small-solve warps across SMs,
 // sorting only inside 256-qp blocks, and a persistent grid-stride launch with
 // 64-256 resident threads per SM all measured slower.)
-constexpr int UPDATE2_BLOCK = 256;
+// Launch shape of the update per lattice class: 256-thread blocks; the FCC
+// class (PMAX 16) at 1 block/SM and up to 255 registers, which measured best
+// (168 registers with 128- or 192-thread blocks measured slower).
+#ifndef CP_U2_SMALL_BLOCK
+#define CP_U2_SMALL_BLOCK 256
+#endif
+#ifndef CP_U2_SMALL_MINB
+#define CP_U2_SMALL_MINB 1
+#endif
+// threads per block of the update for a lattice class (PMAX)
+constexpr int update2_block(int pmax) { return pmax <= 16 ? CP_U2_SMALL_BLOCK : 256; }
 // Resident blocks per SM the compiler sizes registers for: 1 (up to 255
 // registers) for the small FCC-class solve, 2 (128 registers, twice the warps
 // to hide local-memory latency, more spills) for the BCC/HCP classes, whose
 // longer solves gain more from the extra warps than they lose to the spills
 // (measured per class).
-constexpr int update2_min_blocks(int pmax) { return pmax <= 16 ? 1 : 2; }
+constexpr int update2_min_blocks(int pmax) { return pmax <= 16 ? CP_U2_SMALL_MINB : 2; }
 
 template <int PMAX, class FSrc>
 __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, const GroupDev& g, const FSrc& fs,
@@ -278,17 +288,18 @@ __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, cons
 }
 
 template <int PMAX, class FSrc>
-__global__ void __launch_bounds__(UPDATE2_BLOCK, update2_min_blocks(PMAX))
+__global__ void __launch_bounds__(update2_block(PMAX), update2_min_blocks(PMAX))
     update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs, const int* __restrict__ perm, int64_t m,
                    int flag, double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
                    double* __restrict__ stage, int32_t* __restrict__ status, int32_t* __restrict__ stats,
                    double* __restrict__ keepF, double* __restrict__ keepT, int lattice_id) {
-    // per-thread rotated-stiffness slots, entry e of thread t at sD2[e * UPDATE2_BLOCK + t]
-    __shared__ double sD2[21 * UPDATE2_BLOCK];
+    // per-thread rotated-stiffness slots, entry e of thread t at sD2[e * BLOCK + t]
+    constexpr int BLOCK = update2_block(PMAX);
+    __shared__ double sD2[21 * BLOCK];
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j < m)
         update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
-                          lattice_id, sD2 + threadIdx.x, UPDATE2_BLOCK);
+                          lattice_id, sD2 + threadIdx.x, BLOCK);
 }
 
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P
