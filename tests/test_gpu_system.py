@@ -142,3 +142,21 @@ def test_device_system_errors(cuda_lib):
     assert info["converged"] and info["iterations"] == 0
     assert np.abs(be.get_displacement()).max() == 0.0
     be.close()
+
+
+def test_device_newton_hcp_twinning_deck(cuda_lib):
+    """The reference's hcp/compression deck (twin systems, twin reorientation,
+    F_e / F_r feedback) through the device loop: same rows as the host-solve
+    loop and within 1e-3 of the golden curve over the first increments."""
+    n_inc = 12
+    fx = "tests/golden/kat_hcp_compression.npz"
+    hh, d = H.kat_setup(fx, _gpu_factory, M.material_from_deck)
+    hd, _ = H.kat_setup(fx, _gpu_factory, M.material_from_deck, device_system=True)
+    rh = hh.run(n_inc)
+    rd = hd.run(n_inc)
+    assert all(i["converged"] for i in hd.solve_info)
+    assert rel_err(rd[:, :12], rh[:, :12]) < 1e-6
+    err = H.golden_errors(rd, d["golden"], n_inc)
+    assert err["stress"] < 1e-3 and err["strain"] < 1e-3, err
+    hh.be.close()
+    hd.be.close()
