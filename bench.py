@@ -126,11 +126,19 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def wait_first(self, timeout=3.0):
+        """Until nvidia-smi has printed its first sample (bounded)."""
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.02)
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
-    def stop(self):
+    def stop(self, window=None):
+        """Summary of the samples read inside window = (t0, t1) (perf_counter
+        seconds; one sampling interval of slack at the end), or all."""
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -140,7 +148,8 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = [ln for t, ln in self.lines if window is None or window[0] <= t <= window[1] + 0.15]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -258,18 +267,22 @@ def ours(args):
     def step():
         h.update_device(Fn.data_ptr(), 1, 0.0, 0.0, P.data_ptr(), None, dPdF.data_ptr(), status.data_ptr())
 
+    # the clock sampler starts before the warm-up (nvidia-smi needs a moment
+    # to start) and keeps only the samples read during the timed steps
+    clocks = ClockSampler(local)
+    clocks.start()
+    clocks.wait_first()
     for _ in range(args.warmup):
         step()
     h.synchronize()
     st = status.cpu().numpy()
     bad = int(np.count_nonzero(st & capi.CP_QP_ERROR_MASK))
 
-    clocks = ClockSampler(local)
     if world > 1:
         dist.barrier()
     h.synchronize()
     h.set_timing(True)
-    clocks.start()
+    t_begin = time.perf_counter()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
@@ -278,7 +291,7 @@ def ours(args):
             step()
         e1.record(stream)
     e1.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop((t_begin, time.perf_counter()))
     elapsed_ms = e0.elapsed_time(e1)
     timing = h.get_timing()
     h.set_timing(False)
