@@ -384,6 +384,7 @@ def ours(args):
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, parity = cpu_leg(args, h, Fn, P, dPdF, lid, rod)
+    asm = assembly_leg(args, local) if (world == 1 and not args.no_assembly) else None
     rve = rve_leg(args, local) if (world == 1 and not args.no_rve) else None
 
     line = {
@@ -411,6 +412,7 @@ def ours(args):
         "qp_error_flags": bad,
         "cpu_baseline": cpu,
         "parity": parity,
+        "assembly": asm,
         "rve": rve,
     }
     if rank == 0:
@@ -458,6 +460,102 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
     cpu = {"value": n_s / dt, "unit": "qp-updates/s", "cores": threads, "kind": "port",
            "sample": f"first {n_s} qps of the workload (GPU's history, same F), one flag-1 update"}
     return cpu, parity
+
+
+# --------------------------------------------------------------------- assembly
+ASM_N = 64  # 64^3 cells = 2^21 qps
+
+
+def assembly_leg(args, device):
+    """Batched getElementalValues (cp_assemble) on a 64^3 Q1 cube whose cells
+    are FCC/BCC/HCP grains shuffled 50/30/20 (seed SEED_LATTICE) with seeded
+    orientations: 10 committed increments of macroscopic loading
+    F <- F (I + 2e-4 G) plus per-node noise, then the next increment's
+    assembly (update with dP/dF, contraction into Ke/Re) timed device-resident
+    (CUDA events) and end to end through cp_assemble with page-locked host
+    U_local / Ke / Re."""
+    import torch
+    from plasticity_b200 import harness as Hm
+    from plasticity_b200.capi import CpHandle, default_options
+    n = ASM_N
+    nc = n ** 3
+    rng = np.random.default_rng(SEED_LOAD + 7)
+    lid = lattice_ids(nc)
+    rod = orientations(nc)
+    h = CpHandle(materials(), default_options(device=device))
+    h.bind_qps(np.repeat(lid, 8), np.repeat(rod, 8, axis=0))
+    grad = Hm.q1_reference_gradients() * n  # [q][a][3], cell size 1/n
+    jxw = np.full(8, 1.0 / (8 * nc))
+    h.bind_mesh(nc, grad, jxw, True)
+    # cell c = i + n (j + n k) (x fastest); its node a at (i, j, k) + (a&1, a>>1&1, a>>2&1)
+    ijk = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)
+    ijk = ijk[np.lexsort((ijk[:, 0], ijk[:, 1], ijk[:, 2]))]
+    off = np.array([[a & 1, (a >> 1) & 1, (a >> 2) & 1] for a in range(8)])
+    cn = ijk[:, None, :] + off[None, :, :]
+    node = cn[..., 0] + (n + 1) * (cn[..., 1] + (n + 1) * cn[..., 2])
+    xyz = np.zeros(((n + 1) ** 3, 3))
+    ii, jj, kk = np.meshgrid(np.arange(n + 1), np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    xyz[(ii + (n + 1) * (jj + (n + 1) * kk)).ravel()] = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], -1) / n
+    Fm = np.eye(3)
+    noise = np.zeros_like(xyz)
+
+    def u_local():
+        u = xyz @ (Fm - np.eye(3)).T + noise
+        return np.ascontiguousarray(u[node].reshape(nc, 24))
+
+    for _ in range(PRIOR_STEPS):
+        Fm = Fm @ (np.eye(3) + AMP * rng.standard_normal((3, 3)))
+        noise += 2e-5 / n * rng.standard_normal(noise.shape)
+        U = u_local().reshape(nc, 8, 3)
+        F = (np.einsum("cai,qaj->cqij", U, grad) + np.eye(3)).reshape(-1, 9)
+        h.update(F, 0)
+        h.commit()
+    Fm = Fm @ (np.eye(3) + AMP * rng.standard_normal((3, 3)))
+    noise += 2e-5 / n * rng.standard_normal(noise.shape)
+    U = u_local()
+    dev = torch.device("cuda", device)
+    Ud = torch.from_numpy(U).to(dev)
+    Ked = torch.empty(nc, 576, dtype=torch.float64, device=dev)
+    Red = torch.empty(nc, 24, dtype=torch.float64, device=dev)
+    Sd = torch.empty(nc * 8, dtype=torch.int32, device=dev)
+    stream = torch.cuda.ExternalStream(h.stream(), device=dev)
+    step = lambda: h.assemble_device(Ud.data_ptr(), 0.0, 0.0, Ked.data_ptr(), Red.data_ptr(), Sd.data_ptr())
+    for _ in range(args.warmup):
+        step()
+    h.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    plastic = float((h.stats()[:, 1] > 0).mean())
+    hU = torch.empty(nc, 24, dtype=torch.float64, pin_memory=True)
+    hU.copy_(torch.from_numpy(U))
+    hK = torch.empty(nc, 576, dtype=torch.float64, pin_memory=True)
+    hR = torch.empty(nc, 24, dtype=torch.float64, pin_memory=True)
+    hS = torch.empty(nc * 8, dtype=torch.int32, pin_memory=True)
+    import ctypes as C
+    dp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))
+    ip = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_int32))
+    call = lambda: h.lib.cp_assemble(h.h, dp(hU), 0.0, 0.0, dp(hK), dp(hR), ip(hS))
+    for _ in range(args.warmup):
+        assert call() == 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        assert call() == 0
+    e2e_ms = 1e3 * (time.perf_counter() - t0) / args.steps
+    same = bool(torch.equal(hK, Ked.cpu()) and torch.equal(hR, Red.cpu()))
+    h.close()
+    return {"workload": "64^3 Q1 cells (2^21 qps), FCC/BCC/HCP grains 50/30/20, 10 prior increments, flag-1 "
+                        "update + Ke/Re contraction per step",
+            "cells": nc, "ms_per_step": ms, "elements_per_s": nc / (ms * 1e-3),
+            "qp_updates_per_s": 8 * nc / (ms * 1e-3), "plastic_qp_fraction": plastic,
+            "e2e": {"ms_per_step": e2e_ms, "elements_per_s": nc / (e2e_ms * 1e-3),
+                    "h2d_bytes_per_step": 8 * 24 * nc, "d2h_bytes_per_step": 8 * 600 * nc + 4 * 8 * nc,
+                    "matches_device_call": same}}
 
 
 # --------------------------------------------------------------------- RVE solve
@@ -542,6 +640,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain thread-per-qp kernel")
     ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
+    ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -921,7 +921,7 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
             sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status, nullptr,
                                 nullptr);
         contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
-            h->d_stage, h->d_gradN, h->uniform, h->n_cells, d_Ke, d_Re);
+            h->d_stage, h->d_gradN, h->uniform, 0, h->n_cells, d_Ke, d_Re);
         CK(h, cudaGetLastError());
         return CP_OK;
     }
@@ -955,12 +955,52 @@ int cp_assemble(cp_handle* h, const double* h_U, double F_e, double F_r, double*
             cudaMalloc(&h->d_Re, sizeof(double) * 24 * nc) != cudaSuccess)
             return fail(h, CP_E_NOMEM, "cp_assemble: allocation failed");
     }
-    CK(h, cudaMemcpyAsync(h->d_U, h_U, sizeof(double) * 24 * nc, cudaMemcpyHostToDevice, h->stream));
-    if (int rc = cp_assemble_device(h, h->d_U, F_e, F_r, h->d_Ke, h->d_Re, h->d_status)) return rc;
-    CK(h, cudaMemcpyAsync(h_Ke, h->d_Ke, sizeof(double) * 576 * nc, cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaMemcpyAsync(h_Re, h->d_Re, sizeof(double) * 24 * nc, cudaMemcpyDeviceToHost, h->stream));
-    if (h_status)
-        CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * h->n_qp, cudaMemcpyDeviceToHost, h->stream));
+    if (h->opts.plain_kernel) {
+        CK(h, cudaMemcpyAsync(h->d_U, h_U, sizeof(double) * 24 * nc, cudaMemcpyHostToDevice, h->stream));
+        if (int rc = cp_assemble_device(h, h->d_U, F_e, F_r, h->d_Ke, h->d_Re, h->d_status)) return rc;
+        CK(h, cudaMemcpyAsync(h_Ke, h->d_Ke, sizeof(double) * 576 * nc, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(h_Re, h->d_Re, sizeof(double) * 24 * nc, cudaMemcpyDeviceToHost, h->stream));
+        if (h_status)
+            CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * h->n_qp, cudaMemcpyDeviceToHost,
+                                  h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        return CP_OK;
+    }
+    if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_assemble: staging allocation failed");
+    // caller-order chunks of cells (as cp_update): U in on s_in, the sorted
+    // update of the chunk's qps and its contraction on the compute stream, Ke,
+    // Re and status out on s_out while the next chunk computes
+    const FromMesh fm{h->d_U, h->d_gradN, h->d_JxW, h->uniform};
+    const int C = chunks_for(h->n_qp);
+    for (int c = 0; c < C; ++c) {
+        const int64_t c0 = nc * c / C, c1 = nc * (c + 1) / C, ncc = c1 - c0;
+        if (ncc <= 0) continue;
+        CK(h, cudaMemcpyAsync(h->d_U + 24 * c0, h_U + 24 * c0, sizeof(double) * 24 * ncc, cudaMemcpyHostToDevice,
+                              h->s_in));
+        CK(h, cudaEventRecord(h->ev_in[c], h->s_in));
+        CK(h, cudaStreamWaitEvent(h->stream, h->ev_in[c], 0));
+        for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+            const auto& q = h->groups[gi].qp_host;
+            const int64_t i0 = std::lower_bound(q.begin(), q.end(), 8 * c0) - q.begin();
+            const int64_t i1 = std::lower_bound(q.begin(), q.end(), 8 * c1) - q.begin();
+            sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, h->d_status, nullptr,
+                                nullptr, i0, i1 - i0);
+        }
+        contract_kernel<<<blocks_for(ncc, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
+            h->d_stage, h->d_gradN, h->uniform, c0, c1, h->d_Ke, h->d_Re);
+        CK(h, cudaGetLastError());
+        CK(h, cudaEventRecord(h->ev_done[c], h->stream));
+        CK(h, cudaStreamWaitEvent(h->s_out, h->ev_done[c], 0));
+        CK(h, cudaMemcpyAsync(h_Ke + 576 * c0, h->d_Ke + 576 * c0, sizeof(double) * 576 * ncc, cudaMemcpyDeviceToHost,
+                              h->s_out));
+        CK(h, cudaMemcpyAsync(h_Re + 24 * c0, h->d_Re + 24 * c0, sizeof(double) * 24 * ncc, cudaMemcpyDeviceToHost,
+                              h->s_out));
+        if (h_status)
+            CK(h, cudaMemcpyAsync(h_status + 8 * c0, h->d_status + 8 * c0, sizeof(int32_t) * 8 * ncc,
+                                  cudaMemcpyDeviceToHost, h->s_out));
+    }
+    CK(h, cudaStreamSynchronize(h->s_out));
     CK(h, cudaStreamSynchronize(h->stream));
     return CP_OK;
 }

@@ -304,23 +304,25 @@ __global__ void __launch_bounds__(update2_block(PMAX), update2_min_blocks(PMAX))
 
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P
 // and JxW*dP/dF of the cell's 8 qps: thread (cell, node a) writes rows
-// 3a..3a+2 of Ke and Re.  Cells are in caller order; CONTRACT_CELLS per block.
+// 3a..3a+2 of Ke and Re.  Cells [cell_begin, cell_end) in caller order;
+// CONTRACT_CELLS per block.
 constexpr int CONTRACT_CELLS = 8;
 __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const double* __restrict__ stage,
                                                                       const double* __restrict__ gradN, int uniform,
-                                                                      int64_t n_cells, double* __restrict__ Ke,
+                                                                      int64_t cell_begin, int64_t cell_end,
+                                                                      double* __restrict__ Ke,
                                                                       double* __restrict__ Re) {
     __shared__ double sd[CONTRACT_CELLS][8 * 90];
     const int tid = threadIdx.x;
     const int lc = tid >> 3, a1 = tid & 7;
-    const int64_t cell0 = (int64_t)blockIdx.x * CONTRACT_CELLS;
+    const int64_t cell0 = cell_begin + (int64_t)blockIdx.x * CONTRACT_CELLS;
     // cooperative, coalesced load of the block's cells' staged values
-    const int64_t ncb = (n_cells - cell0) < CONTRACT_CELLS ? (n_cells - cell0) : CONTRACT_CELLS;
+    const int64_t ncb = (cell_end - cell0) < CONTRACT_CELLS ? (cell_end - cell0) : CONTRACT_CELLS;
     const double* src = stage + cell0 * 720;
     for (int t = tid; t < ncb * 720; t += CONTRACT_CELLS * 8) sd[t / 720][t % 720] = src[t];
     __syncthreads();
     const int64_t cell = cell0 + lc;
-    if (cell >= n_cells) return;
+    if (cell >= cell_end) return;
     const double* g0 = uniform ? gradN : gradN + cell * 192;
     double K[3][24];
     double Rl[3] = {0.0, 0.0, 0.0};
