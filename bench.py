@@ -98,6 +98,13 @@ def max_over_ranks(x: float, device) -> float:
     return float(t.item())
 
 
+def percentiles(ms):
+    """p50 / p95 / p99 / max of per-step times (ms)."""
+    a = np.asarray(ms, dtype=np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
+            "p99": float(np.percentile(a, 99)), "max": float(a.max()), "steps": int(len(a))}
+
+
 def aggregate_value(world: int, n_qp_per_rank: int, steps: int, seconds: float) -> float:
     """Whole-job qp-updates/s: every rank's qps over the slowest rank's time."""
     return world * n_qp_per_rank * steps / seconds
@@ -285,14 +292,17 @@ def ours(args):
     t_begin = time.perf_counter()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with torch.cuda.stream(stream):
         e0.record(stream)
-        for _ in range(args.steps):
+        for k in range(args.steps):
             step()
+            marks[k].record(stream)  # per-step latency (no synchronisation between steps)
         e1.record(stream)
     e1.synchronize()
     clk = clocks.stop((t_begin, time.perf_counter()))
     elapsed_ms = e0.elapsed_time(e1)
+    step_ms = [e0.elapsed_time(marks[0])] + [marks[k - 1].elapsed_time(marks[k]) for k in range(1, args.steps)]
     timing = h.get_timing()
     h.set_timing(False)
     elapsed_ms = max_over_ranks(elapsed_ms, dev)
@@ -372,12 +382,15 @@ def ours(args):
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
+        call_ms = []
         for _ in range(args.steps):
+            tc = time.perf_counter()
             assert call() == 0
+            call_ms.append(1e3 * (time.perf_counter() - tc))
         dt = max_over_ranks(time.perf_counter() - t0, dev)
         e2e = {"value": aggregate_value(world, n, args.steps, dt), "unit": "qp-updates/s",
                "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": (9 + 81) * 8 * n + 4 * n,
-               "ms_per_step": 1e3 * dt / args.steps}
+               "ms_per_step": 1e3 * dt / args.steps, "latency_ms": percentiles(call_ms)}
 
     # CPU baseline and a live parity check on a bounded sample (rank 0, N=1)
     cpu = None
@@ -396,6 +409,7 @@ def ours(args):
                    "n_qp_per_gpu": n, "stiffness_flag": 1, "parallelism": f"replicas x{world}",
                    "l2": "inputs+outputs+state ~3 GB >> 126 MB L2 (no flush needed)"},
         "clocks": clk,
+        "latency_ms": percentiles(step_ms),
         "e2e": e2e,
         "gpu_launches": args.steps * len(timing) * 4,  # per lattice group: classify, scan, scatter, update
         "roofline": {"bound": "hbm", "kernel": f"update_kernel[{lat_name}]", "achieved": by / (dom_ms * 1e-3) / 1e9,
