@@ -642,6 +642,41 @@ def rve_leg(args, device):
     return out
 
 
+def rve_large_leg(args, device, increments=2):
+    """The device Newton loop at the size of the 48^3 FCC RVE (110,592 cells,
+    884,736 qps, 352,947 dofs; 200 Voronoi grains: nearest of 200 seeded
+    points, seeded orientations; x-tension to 5 % in 50 increments): set-up
+    time, then wall time per increment (4 Newton iterations and the post-pass)
+    over the first increments and the BiCG iterations per Newton solve."""
+    from plasticity_b200 import harness as Hm
+    from plasticity_b200 import materials as M
+    from plasticity_b200.capi import CpHandle, default_options
+    t0 = time.perf_counter()
+    mesh = Hm.StructuredMesh((48, 48, 48))
+    pts = np.random.default_rng(3).random((200, 3))
+    grain_rod = M.random_rodrigues(np.random.default_rng(4), 200)
+    cc = mesh.cell_centres()
+    d2 = (pts ** 2).sum(1)[None, :] - 2.0 * cc @ pts.T  # |c - p|^2 up to the per-cell constant
+    rod = np.repeat(grain_rod[d2.argmin(axis=1)], 8, axis=0)
+    bc = np.array([[1, 1, 0.0], [1, 2, 0.0], [1, 3, 0.0], [2, 1, 0.05]])
+    be = CpHandle([M.fcc_cu()], default_options(device=device))
+    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+    h = Hm.NewtonHarness(be, mesh, bc, 50, 4, device_system=True)
+    t_setup = time.perf_counter() - t0
+    per_inc = []
+    for _ in range(increments):
+        t1 = time.perf_counter()
+        h.step()
+        per_inc.append(time.perf_counter() - t1)
+    it = [i["iterations"] for i in h.solve_info]
+    ok = all(i["converged"] for i in h.solve_info)
+    be.close()
+    return {"workload": "48^3 Q1 FCC cube, 200 Voronoi grains, x-tension 5 % / 50 increments (first increments)",
+            "cells": mesh.n_cells, "dofs": mesh.n_dofs, "setup_s": t_setup, "seconds_per_increment": per_inc,
+            "bicg_iterations_per_solve": it, "all_converged": ok,
+            "projected_rve_seconds": float(np.mean(per_inc)) * 50}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -655,11 +690,15 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain thread-per-qp kernel")
     ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
+    ap.add_argument("--rve-large", action="store_true", help="only time the 48^3 RVE's first increments")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if args.rve_large:
+        print(json.dumps({"rve_large": rve_large_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        return 0
     return ours(args)
 
 

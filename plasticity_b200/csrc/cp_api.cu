@@ -321,6 +321,7 @@ struct cp_handle {
         int64_t* d_con = nullptr;               // constrained dofs
         unsigned char* d_cmask = nullptr;       // n_dofs
         double *d_vals = nullptr, *d_Ke = nullptr, *d_Re = nullptr, *d_Ul = nullptr, *d_duc = nullptr;
+        double* d_valsT = nullptr;              // K^T's values in K's pattern (per solve)
         double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
         double *d_sc = nullptr, *d_partial = nullptr;
         double* d_fpartial = nullptr;           // per-block partials of the fused iteration (n_dofs / 8 + 64)
@@ -428,6 +429,7 @@ void free_system(cp_handle* h) {
     cudaFree(y.d_con);
     cudaFree(y.d_cmask);
     cudaFree(y.d_vals);
+    cudaFree(y.d_valsT);
     cudaFree(y.d_Ke);
     cudaFree(y.d_Re);
     cudaFree(y.d_Ul);
@@ -1381,6 +1383,7 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
               cudaMalloc(&y.d_con, sizeof(int64_t) * std::max<int64_t>(n_constrained, 1)) == cudaSuccess &&
               cudaMalloc(&y.d_cmask, n_dofs) == cudaSuccess &&
               cudaMalloc(&y.d_vals, sizeof(double) * nnz) == cudaSuccess &&
+              cudaMalloc(&y.d_valsT, sizeof(double) * nnz) == cudaSuccess &&
               cudaMalloc(&y.d_Ke, sizeof(double) * 576 * nc) == cudaSuccess &&
               cudaMalloc(&y.d_Re, sizeof(double) * 24 * nc) == cudaSuccess &&
               cudaMalloc(&y.d_Ul, sizeof(double) * 24 * nc) == cudaSuccess &&
@@ -1478,7 +1481,7 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
         fbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
                                                               s.d_done, s.d_info);
         fbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
-            s.d_row_ptr, s.d_col, s.d_vals, s.d_tpos, v(V_P), v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
+            s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_P), v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
             s.d_ticket + 1, done);
         fbicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_P), v(V_Q), v(V_QT), v(V_DINV), n,
                                                                sv.rel_tolerance, sv.precond_norm, v(V_X), v(V_RES),
@@ -1579,6 +1582,8 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
     condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
     jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
+    transpose_values_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_tpos, s.nnz,
+                                                                                          s.d_valsT);
     // Krylov solve from x = 0: r = r~ = rhs
     CK(h, cudaMemsetAsync(v(V_X), 0, sizeof(double) * n, h->stream));
     copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(V_RES));

@@ -237,6 +237,13 @@ __global__ void scale_kernel(const double* __restrict__ a, const double* __restr
     if (i < n) y[i] = a[i] * dinv[i];
 }
 
+// valsT[p] = vals[tpos[p]]: the values of K^T in K's pattern
+__global__ void transpose_values_kernel(const double* __restrict__ vals, const int64_t* __restrict__ tpos, int64_t nnz,
+                                        double* __restrict__ valsT) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < nnz) valsT[p] = vals[tpos[p]];
+}
+
 // dinv[i] = 1 / K_ii (zero diagonal -> 1, the row is then left unpreconditioned)
 __global__ void jacobi_setup_kernel(const double* __restrict__ vals, const int64_t* __restrict__ diag_pos, int64_t n,
                                     double* __restrict__ dinv) {
@@ -321,10 +328,11 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_dir_kernel(
 }
 
 // (3) q = K p and q~ = K^T p~ (a warp per row, both in one pass over the
-// row); den = p~ . q
+// row; valsT[k] = K value of the transposed entry, gathered once per solve);
+// den = p~ . q
 __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv_kernel(
     const int64_t* __restrict__ row_ptr, const int* __restrict__ col, const double* __restrict__ vals,
-    const int64_t* __restrict__ tpos, const double* __restrict__ p, const double* __restrict__ pt, int64_t n,
+    const double* __restrict__ valsT, const double* __restrict__ p, const double* __restrict__ pt, int64_t n,
     double* __restrict__ q, double* __restrict__ qt, double* __restrict__ sc, double* __restrict__ partial,
     unsigned int* __restrict__ ticket, const int* __restrict__ done) {
     if (*done) return;
@@ -336,7 +344,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv_kernel(
         for (int64_t k = row_ptr[row] + lane; k < row_ptr[row + 1]; k += 32) {
             const int c = col[k];
             s += vals[k] * p[c];
-            st += vals[tpos[k]] * pt[c];
+            st += valsT[k] * pt[c];
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

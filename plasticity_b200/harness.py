@@ -81,12 +81,15 @@ class StructuredMesh:
         gref = q1_reference_gradients()
         self.grad_N = gref / self.h  # uniform mesh: [q][a][3]
         self.JxW = np.full(8, np.prod(self.h) / 8.0)
-        self._build_pattern()
+        self._pattern = False  # the host CSR pattern, built on first use (the device system needs none)
 
     def cell_centres(self):
         return self.node_xyz[self.cell_nodes].mean(axis=1)
 
     def _build_pattern(self):
+        if self._pattern:
+            return
+        self._pattern = True
         rows = np.repeat(self.cell_dofs, 24, axis=1).ravel()
         cols = np.tile(self.cell_dofs, (1, 24)).ravel()
         lin = rows * self.n_dofs + cols
@@ -100,6 +103,7 @@ class StructuredMesh:
         self._rows = r
 
     def assemble_matrix(self, Ke):
+        self._build_pattern()
         data = np.bincount(self._pos, weights=np.asarray(Ke).ravel(), minlength=self._nnz)
         return sp.csr_matrix((data, self._indices, self._indptr), shape=(self.n_dofs, self.n_dofs))
 
@@ -190,7 +194,7 @@ class NewtonHarness:
         mask = np.zeros(mesh.n_dofs, dtype=bool)
         mask[self.cdofs] = True
         self.cmask = mask
-        self._zero_entries = mask[mesh._rows] | mask[mesh._indices]
+        self._zero_entries = None  # host condensation mask, built on first host solve
         self._diag = None
         backend.bind_mesh(mesh.n_cells, mesh.grad_N, mesh.JxW, True)
         if device_system:
@@ -202,6 +206,9 @@ class NewtonHarness:
         du_full = np.zeros(self.mesh.n_dofs)
         du_full[self.cdofs] = duc
         rhs = R - K @ du_full
+        if self._zero_entries is None:
+            self.mesh._build_pattern()
+            self._zero_entries = self.cmask[self.mesh._rows] | self.cmask[self.mesh._indices]
         K = K.copy()
         K.data[self._zero_entries] = 0.0
         K = K + sp.diags(self.cmask.astype(float))
