@@ -650,8 +650,7 @@ def rve_large_leg(args, device, increments=2):
     over the first increments and the BiCG iterations per Newton solve."""
     from plasticity_b200 import harness as Hm
     from plasticity_b200 import materials as M
-    from plasticity_b200.capi import CpHandle, default_options
-    t0 = time.perf_counter()
+    from plasticity_b200.capi import CpHandle, default_options, default_solver
     mesh = Hm.StructuredMesh((48, 48, 48))
     pts = np.random.default_rng(3).random((200, 3))
     grain_rod = M.random_rodrigues(np.random.default_rng(4), 200)
@@ -659,22 +658,26 @@ def rve_large_leg(args, device, increments=2):
     d2 = (pts ** 2).sum(1)[None, :] - 2.0 * cc @ pts.T  # |c - p|^2 up to the per-cell constant
     rod = np.repeat(grain_rod[d2.argmin(axis=1)], 8, axis=0)
     bc = np.array([[1, 1, 0.0], [1, 2, 0.0], [1, 3, 0.0], [2, 1, 0.05]])
-    be = CpHandle([M.fcc_cu()], default_options(device=device))
-    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
-    h = Hm.NewtonHarness(be, mesh, bc, 50, 4, device_system=True)
-    t_setup = time.perf_counter() - t0
-    per_inc = []
-    for _ in range(increments):
-        t1 = time.perf_counter()
-        h.step()
-        per_inc.append(time.perf_counter() - t1)
-    it = [i["iterations"] for i in h.solve_info]
-    ok = all(i["converged"] for i in h.solve_info)
-    be.close()
-    return {"workload": "48^3 Q1 FCC cube, 200 Voronoi grains, x-tension 5 % / 50 increments (first increments)",
-            "cells": mesh.n_cells, "dofs": mesh.n_dofs, "setup_s": t_setup, "seconds_per_increment": per_inc,
-            "bicg_iterations_per_solve": it, "all_converged": ok,
-            "projected_rve_seconds": float(np.mean(per_inc)) * 50}
+    out = {"workload": "48^3 Q1 FCC cube, 200 Voronoi grains, x-tension 5 % / 50 increments (first increments)",
+           "cells": mesh.n_cells, "dofs": mesh.n_dofs}
+    for pc, name in ((0, "jacobi"), (1, "node_block")):
+        t0 = time.perf_counter()
+        be = CpHandle([M.fcc_cu()], default_options(device=device))
+        be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+        h = Hm.NewtonHarness(be, mesh, bc, 50, 4, device_system=True, solver=default_solver(precond=pc))
+        t_setup = time.perf_counter() - t0
+        per_inc = []
+        for _ in range(increments):
+            t1 = time.perf_counter()
+            h.step()
+            per_inc.append(time.perf_counter() - t1)
+        out[name] = {"setup_s": t_setup, "seconds_per_increment": per_inc,
+                     "bicg_iterations_per_solve": [i["iterations"] for i in h.solve_info],
+                     "all_converged": all(i["converged"] for i in h.solve_info),
+                     "final_stress_xx_mpa": float(h.rows[-1][6]),
+                     "projected_rve_seconds": float(np.mean(per_inc)) * 50}
+        be.close()
+    return out
 
 
 def main():

@@ -272,12 +272,17 @@ int cp_get_displacement(cp_handle* h, double* h_u);
 
 #define CP_SOLVER_BICG 0     /* PETScWrappers::SolverBiCG, the reference's solver */
 #define CP_SOLVER_BICGSTAB 1 /* BiCGStab (right Jacobi preconditioning) */
+#define CP_PRECOND_JACOBI 0     /* PETScWrappers::PreconditionJacobi, the reference's */
+#define CP_PRECOND_NODE_BLOCK 1 /* inverse of each node's 3x3 diagonal block (BiCG, precond_norm 0) */
 typedef struct cp_solver_t {
     int32_t kind;           /* CP_SOLVER_* */
     int32_t max_iterations; /* "Maximum linear solver iterations" (decks: 50000) */
     double rel_tolerance;   /* "Relative linear solver tolerance": stop at ||r|| <= tol ||b|| */
     int32_t precond_norm;   /* 0: true residual ||b - K du||; 1: ||M^-1 r|| (PETSc's BiCG default) */
     int32_t check_every;    /* iterations queued between host checks of convergence (0: 8) */
+    int32_t precond;        /* CP_PRECOND_* (the node blocks need the three components of every
+                               node among one cell's local dofs 3a..3a+2, as cp_bind_dofs takes them) */
+    int32_t reserved;
 } cp_solver_t;
 typedef struct cp_solve_info_t {
     int32_t iterations; /* Krylov iterations to convergence (or the cap) */
@@ -287,7 +292,7 @@ typedef struct cp_solve_info_t {
     double rhs_norm;      /* ||b|| of the condensed system */
     double residual_norm; /* the tested residual norm at exit */
 } cp_solve_info_t;
-int cp_solver_default(cp_solver_t* solver); /* BiCG, 50000, 1e-10, true residual */
+int cp_solver_default(cp_solver_t* solver); /* BiCG, Jacobi, 50000, 1e-10, true residual */
 
 /*
  * One Newton iteration on the device (solveNonLinearSystem.cc:14-81, one

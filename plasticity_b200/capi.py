@@ -93,6 +93,8 @@ class CpSolver(C.Structure):
         ("rel_tolerance", C.c_double),
         ("precond_norm", C.c_int32),
         ("check_every", C.c_int32),
+        ("precond", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -109,12 +111,15 @@ class CpSolveInfo(C.Structure):
 
 CP_SOLVER_BICG = 0
 CP_SOLVER_BICGSTAB = 1
+CP_PRECOND_JACOBI = 0
+CP_PRECOND_NODE_BLOCK = 1
 
 
 def default_solver(**kw) -> CpSolver:
     """The reference decks' settings: BiCG, 50000 iterations, 1e-10 x ||b||."""
     s = CpSolver()
     s.kind, s.max_iterations, s.rel_tolerance, s.precond_norm, s.check_every = CP_SOLVER_BICG, 50000, 1e-10, 0, 8
+    s.precond = CP_PRECOND_JACOBI
     for k, v in kw.items():
         setattr(s, k, v)
     return s

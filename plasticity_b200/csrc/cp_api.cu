@@ -322,6 +322,9 @@ struct cp_handle {
         unsigned char* d_cmask = nullptr;       // n_dofs
         double *d_vals = nullptr, *d_Ke = nullptr, *d_Re = nullptr, *d_Ul = nullptr, *d_duc = nullptr;
         double* d_valsT = nullptr;              // K^T's values in K's pattern (per solve)
+        int64_t n_blocks = 0;                   // node blocks (0: unavailable)
+        int64_t *d_blk = nullptr, *d_blkpos = nullptr;  // 3 dofs / 9 entry positions per node block
+        double* d_binv = nullptr;               // inverted 3x3 blocks (per solve)
         double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
         double *d_sc = nullptr, *d_partial = nullptr;
         double* d_fpartial = nullptr;           // per-block partials of the fused iteration (n_dofs / 8 + 64)
@@ -330,7 +333,7 @@ struct cp_handle {
         // a block of Krylov iterations captured as CUDA graphs (first block /
         // later blocks), for the solver settings they were captured with
         cudaGraphExec_t g_first = nullptr, g_next = nullptr;
-        int g_kind = -1, g_precond = -1, g_every = 0;
+        int g_kind = -1, g_precond = -1, g_every = 0, g_pc = -1;
         double g_tol = -1.0;
     } sys;
     // averages scratch
@@ -430,6 +433,9 @@ void free_system(cp_handle* h) {
     cudaFree(y.d_cmask);
     cudaFree(y.d_vals);
     cudaFree(y.d_valsT);
+    cudaFree(y.d_blk);
+    cudaFree(y.d_blkpos);
+    cudaFree(y.d_binv);
     cudaFree(y.d_Ke);
     cudaFree(y.d_Re);
     cudaFree(y.d_Ul);
@@ -1345,6 +1351,35 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
     }
     for (int64_t i = 0; i < n_dofs; ++i)
         if (diag[i] < 0) return fail(h, CP_E_ARG, "cp_bind_dofs: a dof belongs to no cell");
+    // node blocks: the three components of a node, local dofs 3a..3a+2 of a
+    // cell; usable when every dof sits in exactly one such triple
+    std::vector<int64_t> blk, blkpos;
+    {
+        std::vector<int64_t> owner(n_dofs, -1);
+        bool ok = true;
+        for (int64_t c = 0; c < nc && ok; ++c)
+            for (int a = 0; a < 8 && ok; ++a) {
+                const int64_t* g = h_cell_dofs + 24 * c + 3 * a;
+                const int64_t b = owner[g[0]];
+                if (b < 0) {
+                    const int64_t nb = (int64_t)blk.size() / 3;
+                    for (int k = 0; k < 3; ++k) {
+                        if (owner[g[k]] >= 0) ok = false;
+                        owner[g[k]] = nb;
+                        blk.push_back(g[k]);
+                    }
+                } else {
+                    for (int k = 0; k < 3; ++k) ok = ok && blk[3 * b + k] == g[k];
+                }
+            }
+        if (ok)
+            for (int64_t b = 0; b < (int64_t)blk.size() / 3; ++b)
+                for (int r = 0; r < 3; ++r)
+                    for (int q = 0; q < 3; ++q) blkpos.push_back(find(blk[3 * b + r], (int)blk[3 * b + q]));
+        else
+            blk.clear();
+    }
+    const int64_t n_blocks = (int64_t)blk.size() / 3;
     // contributions of element entries (cell order within each entry)
     std::vector<int64_t> kptr(nnz + 1, 0), kidx(576 * nc), epos(576 * nc);
     for (int64_t c = 0; c < nc; ++c)
@@ -1371,6 +1406,18 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
     y.n_dofs = n_dofs;
     y.nnz = nnz;
     y.n_con = n_constrained;
+    y.n_blocks = n_blocks;
+    if (n_blocks &&
+        (cudaMalloc(&y.d_blk, sizeof(int64_t) * 3 * n_blocks) != cudaSuccess ||
+         cudaMalloc(&y.d_blkpos, sizeof(int64_t) * 9 * n_blocks) != cudaSuccess ||
+         cudaMalloc(&y.d_binv, sizeof(double) * 9 * n_blocks) != cudaSuccess)) {
+        free_system(h);
+        return fail(h, CP_E_NOMEM, "cp_bind_dofs: device allocation failed");
+    }
+    if (n_blocks) {
+        CK(h, cudaMemcpy(y.d_blk, blk.data(), sizeof(int64_t) * 3 * n_blocks, cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(y.d_blkpos, blkpos.data(), sizeof(int64_t) * 9 * n_blocks, cudaMemcpyHostToDevice));
+    }
     bool ok = cudaMalloc(&y.d_cell_dofs, sizeof(int64_t) * 24 * nc) == cudaSuccess &&
               cudaMalloc(&y.d_row_ptr, sizeof(int64_t) * (n_dofs + 1)) == cudaSuccess &&
               cudaMalloc(&y.d_col, sizeof(int) * nnz) == cudaSuccess &&
@@ -1476,8 +1523,14 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
                                                                v(V_RES), done);
     } else {
         // BiCG in four kernels; the last one also tests convergence
-        fbicg_precond_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_DINV), v(V_RES), v(V_RT), n, v(V_Z), v(V_ZT),
-                                                                  s.d_sc, s.d_fpartial, s.d_ticket + 0, done);
+        if (sv.precond == CP_PRECOND_NODE_BLOCK)
+            fbicg_precond_block_kernel<<<blocks_for(s.n_blocks, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+                s.d_binv, s.d_blk, v(V_RES), v(V_RT), s.n_blocks, v(V_Z), v(V_ZT), s.d_sc, s.d_fpartial,
+                s.d_ticket + 0, done);
+        else
+            fbicg_precond_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_DINV), v(V_RES), v(V_RT), n, v(V_Z),
+                                                                      v(V_ZT), s.d_sc, s.d_fpartial, s.d_ticket + 0,
+                                                                      done);
         fbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
                                                               s.d_done, s.d_info);
         fbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
@@ -1504,7 +1557,7 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
 bool ensure_solve_graphs(cp_handle* h, const cp_solver_t& sv, int every) {
     auto& s = h->sys;
     if (s.g_first && s.g_next && s.g_kind == sv.kind && s.g_precond == sv.precond_norm && s.g_every == every &&
-        s.g_tol == sv.rel_tolerance)
+        s.g_tol == sv.rel_tolerance && s.g_pc == sv.precond)
         return true;
     if (s.g_first) cudaGraphExecDestroy(s.g_first);
     if (s.g_next) cudaGraphExecDestroy(s.g_next);
@@ -1527,6 +1580,7 @@ bool ensure_solve_graphs(cp_handle* h, const cp_solver_t& sv, int every) {
     s.g_precond = sv.precond_norm;
     s.g_every = every;
     s.g_tol = sv.rel_tolerance;
+    s.g_pc = sv.precond;
     return true;
 }
 
@@ -1539,6 +1593,8 @@ int cp_solver_default(cp_solver_t* sv) {
     sv->rel_tolerance = 1.0e-10;
     sv->precond_norm = 0;
     sv->check_every = 8;
+    sv->precond = CP_PRECOND_JACOBI;
+    sv->reserved = 0;
     return CP_OK;
 }
 
@@ -1555,6 +1611,12 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     if ((sv.kind != CP_SOLVER_BICG && sv.kind != CP_SOLVER_BICGSTAB) || sv.max_iterations < 1 ||
         !(sv.rel_tolerance >= 0.0))
         return fail(h, CP_E_ARG, "cp_newton_iteration: bad solver settings");
+    if (sv.precond != CP_PRECOND_JACOBI && sv.precond != CP_PRECOND_NODE_BLOCK)
+        return fail(h, CP_E_ARG, "cp_newton_iteration: unknown preconditioner");
+    if (sv.precond == CP_PRECOND_NODE_BLOCK && (sv.kind != CP_SOLVER_BICG || sv.precond_norm))
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: node blocks need BiCG with the true-residual test");
+    if (sv.precond == CP_PRECOND_NODE_BLOCK && !s.n_blocks)
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: the dof map has no node blocks");
     if (int rc = check_device(h)) return rc;
     if (int rc = ensure_staging(h, false)) return rc;
     const int64_t n = s.n_dofs, nc = h->n_cells;
@@ -1582,6 +1644,9 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
     condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
     jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
+    if (sv.precond == CP_PRECOND_NODE_BLOCK)
+        block_setup_kernel<<<blocks_for(s.n_blocks, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_blkpos,
+                                                                                             s.n_blocks, s.d_binv);
     transpose_values_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_tpos, s.nnz,
                                                                                           s.d_valsT);
     // Krylov solve from x = 0: r = r~ = rhs

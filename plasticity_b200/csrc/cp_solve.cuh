@@ -237,6 +237,39 @@ __global__ void scale_kernel(const double* __restrict__ a, const double* __restr
     if (i < n) y[i] = a[i] * dinv[i];
 }
 
+// binv[9 b..] = inverse of node b's 3x3 diagonal block of K (entries at
+// blkpos[9 b + 3 a + c]), by the adjugate; a singular or non-finite block
+// falls back to the inverse of its diagonal (1 for a zero diagonal entry)
+__global__ void block_setup_kernel(const double* __restrict__ vals, const int64_t* __restrict__ blkpos, int64_t nb,
+                                   double* __restrict__ binv) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    double m[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) m[e] = vals[blkpos[9 * b + e]];
+    const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
+    const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+    double* o = binv + 9 * b;
+    if (det != 0.0 && isfinite(det)) {
+        const double r = 1.0 / det;
+        o[0] = c00 * r;
+        o[1] = (m[2] * m[7] - m[1] * m[8]) * r;
+        o[2] = (m[1] * m[5] - m[2] * m[4]) * r;
+        o[3] = c01 * r;
+        o[4] = (m[0] * m[8] - m[2] * m[6]) * r;
+        o[5] = (m[2] * m[3] - m[0] * m[5]) * r;
+        o[6] = c02 * r;
+        o[7] = (m[1] * m[6] - m[0] * m[7]) * r;
+        o[8] = (m[0] * m[4] - m[1] * m[3]) * r;
+    } else {
+#pragma unroll
+        for (int e = 0; e < 9; ++e) o[e] = 0.0;
+        o[0] = m[0] != 0.0 ? 1.0 / m[0] : 1.0;
+        o[4] = m[4] != 0.0 ? 1.0 / m[4] : 1.0;
+        o[8] = m[8] != 0.0 ? 1.0 / m[8] : 1.0;
+    }
+}
+
 // valsT[p] = vals[tpos[p]]: the values of K^T in K's pattern
 __global__ void transpose_values_kernel(const double* __restrict__ vals, const int64_t* __restrict__ tpos, int64_t nnz,
                                         double* __restrict__ valsT) {
@@ -302,6 +335,33 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_precond_kernel(
         z[i] = a;
         zt[i] = b;
         v = a * rt[i];
+    }
+    last_block_sum(v, partial, ticket, sc + SC_RHO);
+}
+
+// (1, node blocks) z = B^-1 r and z~ = B^-T r~ per node (dofs blk[3 b..]);
+// rho = z . r~
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_precond_block_kernel(
+    const double* __restrict__ binv, const int64_t* __restrict__ blk, const double* __restrict__ r,
+    const double* __restrict__ rt, int64_t nb, double* __restrict__ z, double* __restrict__ zt,
+    double* __restrict__ sc, double* __restrict__ partial, unsigned int* __restrict__ ticket,
+    const int* __restrict__ done) {
+    if (*done) return;
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (b < nb) {
+        const int64_t g[3] = {blk[3 * b], blk[3 * b + 1], blk[3 * b + 2]};
+        const double* B = binv + 9 * b;
+        const double r0 = r[g[0]], r1 = r[g[1]], r2 = r[g[2]];
+        const double t0 = rt[g[0]], t1 = rt[g[1]], t2 = rt[g[2]];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double za = B[3 * a] * r0 + B[3 * a + 1] * r1 + B[3 * a + 2] * r2;
+            const double zta = B[a] * t0 + B[3 + a] * t1 + B[6 + a] * t2;
+            z[g[a]] = za;
+            zt[g[a]] = zta;
+            v += za * (a == 0 ? t0 : (a == 1 ? t1 : t2));
+        }
     }
     last_block_sum(v, partial, ticket, sc + SC_RHO);
 }

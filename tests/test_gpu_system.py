@@ -8,8 +8,8 @@ import pytest
 
 from plasticity_b200 import harness as H
 from plasticity_b200 import materials as M
-from plasticity_b200.capi import (CP_SOLVER_BICG, CP_SOLVER_BICGSTAB, CpError, CpHandle, default_options,
-                                  default_solver)
+from plasticity_b200.capi import (CP_PRECOND_NODE_BLOCK, CP_SOLVER_BICG, CP_SOLVER_BICGSTAB, CpError, CpHandle,
+                                  default_options, default_solver)
 from tests._parity import rel_err
 
 pytestmark = pytest.mark.gpu
@@ -88,16 +88,24 @@ def test_device_newton_iteration_solves_the_condensed_system(cuda_lib):
     h = H.NewtonHarness(be, mesh, bc, 8, 4, device_system=True)
     h.run(2)
     u0 = be.get_displacement()
-    for kind in (CP_SOLVER_BICG, CP_SOLVER_BICGSTAB):
+    iters = {}
+    for kind, pc in ((CP_SOLVER_BICG, 0), (CP_SOLVER_BICGSTAB, 0), (CP_SOLVER_BICG, CP_PRECOND_NODE_BLOCK)):
         be.set_displacement(u0)
         Ke, Re, _ = be.assemble(u0[mesh.cell_dofs], h.F_e, h.F_r)
         K, R = mesh.assemble_matrix(Ke), mesh.assemble_vector(Re)
         du_ref = h._solve(K, R, h.cvals)
-        info = be.newton_iteration(h.cvals, h.F_e, h.F_r, default_solver(kind=kind))
+        info = be.newton_iteration(h.cvals, h.F_e, h.F_r, default_solver(kind=kind, precond=pc))
         du = be.get_displacement() - u0
         assert info["converged"] and info["iterations"] > 0
-        assert np.abs(du - du_ref).max() <= 1e-7 * np.abs(du_ref).max(), kind
+        assert np.abs(du - du_ref).max() <= 1e-7 * np.abs(du_ref).max(), (kind, pc)
         assert np.allclose(du[h.cdofs], h.cvals, rtol=1e-12, atol=1e-15)  # prescribed increments distributed
+        iters[(kind, pc)] = info["iterations"]
+    # the node-block preconditioner needs fewer BiCG iterations than point Jacobi
+    assert iters[(CP_SOLVER_BICG, CP_PRECOND_NODE_BLOCK)] < iters[(CP_SOLVER_BICG, 0)], iters
+    with pytest.raises(CpError):  # node blocks: BiCG with the true-residual test only
+        be.newton_iteration(None, h.F_e, h.F_r, default_solver(kind=CP_SOLVER_BICGSTAB, precond=CP_PRECOND_NODE_BLOCK))
+    with pytest.raises(CpError):
+        be.newton_iteration(None, h.F_e, h.F_r, default_solver(precond=7))
     be.close()
 
 
