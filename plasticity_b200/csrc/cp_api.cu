@@ -1491,11 +1491,11 @@ void sys_dot(cp_handle* h, const double* x, const double* y, int slot, const int
     dot_final_kernel<<<1, SOLVE_BLOCK, 0, h->stream>>>(s.d_partial, s.d_sc + slot, done);
 }
 
-void sys_spmv(cp_handle* h, const double* x, double* y, bool transpose, const int* done) {
+void sys_spmv(cp_handle* h, const double* x, double* y, const int* done) {
     auto& s = h->sys;
     const int64_t threads = 32 * s.n_dofs;
-    spmv_kernel<<<blocks_for(threads, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
-        s.d_row_ptr, s.d_col, s.d_vals, transpose ? s.d_tpos : nullptr, x, s.n_dofs, y, done);
+    spmv_kernel<<<blocks_for(threads, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_vals, x,
+                                                                              s.n_dofs, y, done);
 }
 
 // one Krylov iteration of the chosen method (queued, no host sync)
@@ -1511,12 +1511,12 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
         bicgstab_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_RES), v(V_Q), n, first, v(V_P),
                                                                  s.d_done, s.d_info);
         scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_P), v(V_DINV), n, v(V_PH), done);
-        sys_spmv(h, v(V_PH), v(V_Q), false, done);  // v
+        sys_spmv(h, v(V_PH), v(V_Q), done);  // v
         sys_dot(h, v(V_RT), v(V_Q), SC_DEN, done);
         bicgstab_s_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_RES), v(V_Q), n, v(V_S), s.d_done,
                                                                s.d_info);
         scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_S), v(V_DINV), n, v(V_SH), done);
-        sys_spmv(h, v(V_SH), v(V_T), false, done);
+        sys_spmv(h, v(V_SH), v(V_T), done);
         sys_dot(h, v(V_T), v(V_S), SC_TS, done);
         sys_dot(h, v(V_T), v(V_T), SC_TT, done);
         bicgstab_x_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_PH), v(V_SH), v(V_S), v(V_T), n, v(V_X),
@@ -1640,7 +1640,7 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     if (s.n_con)
         constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
                                                                                                   s.n_con, v(V_DC));
-    sys_spmv(h, v(V_DC), v(V_KDC), false, nullptr);
+    sys_spmv(h, v(V_DC), v(V_KDC), nullptr);
     condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
     condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
     jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));

@@ -8,7 +8,7 @@
 //
 // Layout: K is CSR (row_ptr int64, col int32, values FP64), rows = global dofs.
 // The Q1 pattern is structurally symmetric, so tpos[p] (the position of entry
-// (j, i) for entry p = (i, j)) gives K^T products from the same arrays.  Every
+// (j, i) for entry p = (i, j)) turns K's values into K^T's in the same pattern.  Every
 // reduction is two-stage with a fixed block count and a fixed final order, so
 // a solve is deterministic for a given input.
 #pragma once
@@ -73,18 +73,17 @@ __global__ void condense_rhs_kernel(const double* __restrict__ R, const double* 
 
 // ---- sparse products (a warp per row: the row's entries load coalesced) ---
 
-// y = K x, or y = K^T x when tpos is given (entry (j,i) of row i at tpos[p])
+// y = K x
 __global__ void spmv_kernel(const int64_t* __restrict__ row_ptr, const int* __restrict__ col,
-                            const double* __restrict__ vals, const int64_t* __restrict__ tpos,
-                            const double* __restrict__ x, int64_t n, double* __restrict__ y,
-                            const int* __restrict__ done) {
+                            const double* __restrict__ vals, const double* __restrict__ x, int64_t n,
+                            double* __restrict__ y, const int* __restrict__ done) {
     if (done && *done) return;
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
     double s = 0.0;
     for (int64_t p = row_ptr[row] + lane; p < row_ptr[row + 1]; p += 32)
-        s += (tpos ? vals[tpos[p]] : vals[p]) * x[col[p]];
+        s += vals[p] * x[col[p]];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) y[row] = s;
