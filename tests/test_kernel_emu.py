@@ -1,6 +1,8 @@
-"""The CUDA qp kernel source (plasticity_b200/csrc/cp_qp.cuh) compiled for
-the host and run against the oracle: checks the device code path's logic in
-the CPU suite (the GPU tests check the compiled sm_100a build)."""
+"""The CUDA qp kernel source compiled for the host and run against the
+oracle: the optimised update (plasticity_b200/csrc/cp_qp2.cuh, qp_update2)
+and the plain form (cp_qp.cuh, qp_update; cp_options_t.plain_kernel).  Checks
+the device code path's logic in the CPU suite (the GPU tests check the
+compiled sm_100a build)."""
 import numpy as np
 import pytest
 
@@ -15,8 +17,10 @@ def emu():
     return E
 
 
+@pytest.mark.parametrize("variant", [0, 1], ids=["qp_update2", "qp_update_plain"])
 @pytest.mark.parametrize("lat", ["fcc", "bcc", "hcp"])
-def test_kernel_source_matches_oracle(oracle_lib, emu, lat):
+def test_kernel_source_matches_oracle(oracle_lib, emu, lat, variant):
+    emu.lib().emu_set_variant(variant)
     mat = {"fcc": M.fcc_cu, "bcc": M.bcc_48, "hcp": M.hcp_mg}[lat]()
     rng = np.random.default_rng(5)
     n = 400
@@ -37,6 +41,7 @@ def test_kernel_source_matches_oracle(oracle_lib, emu, lat):
     assert rel_err(Pe[ok], Po[ok]) < TOL and rel_err(De[ok], Do[ok]) < TOL
     for f in ("Fp_iter", "s_iter"):
         assert rel_err(eb.get_state(f)[ok], ob.get_state(f)[ok]) < TOL
+    emu.lib().emu_set_variant(0)
 
 
 def test_kernel_source_general_caps(oracle_lib, emu):
