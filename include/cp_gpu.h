@@ -146,7 +146,9 @@ int64_t cp_num_qps(const cp_handle* h);
  * written when stiffness_flag == 1), h_status (n_qp status bits).
  * F_e / F_r are the previous increment's volume-averaged twin quantities
  * (updateAfterIncrement.cc:719-720) used by the twin-reorientation threshold.
- * Synchronous: returns when the outputs are in host memory.
+ * Synchronous: returns when the outputs are in host memory.  Batches above
+ * 2^18 qps run in caller-order chunks whose copies overlap the other chunks'
+ * kernels; page-locked host buffers get the full overlap.
  */
 int cp_update(cp_handle* h, const double* h_F, int32_t stiffness_flag,
               double F_e, double F_r, double* h_P, double* h_T, double* h_dPdF,
@@ -184,7 +186,8 @@ int cp_bind_mesh(cp_handle* h, int64_t n_cells, const double* h_grad_N,
  * F = I + sum_d U_d grad N_d at each qp, calculatePlasticity(...,1), then
  * Re[d] -= gradN_d . P . JxW and Ke[d1][d2] += gradN_d1 . dPdF . gradN_d2 JxW.
  * h_U_local: 24*n_cells; outputs h_Ke 576*n_cells (row-major 24x24, not
- * symmetric), h_Re 24*n_cells.
+ * symmetric), h_Re 24*n_cells.  Synchronous; chunked over cells like
+ * cp_update (copies overlap the kernels of the other chunks).
  */
 int cp_assemble(cp_handle* h, const double* h_U_local, double F_e, double F_r,
                 double* h_Ke, double* h_Re, int32_t* h_status);
