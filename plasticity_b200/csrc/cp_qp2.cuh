@@ -403,12 +403,42 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             if (ng) neg_d |= (1ull << k);
             w.kin[k] = ng ? -kin : kin;
         }
-        for (int kj = 0; kj < p_init; ++kj) {
-            const int bsys = w.pa0[kj];
+        // column j of A needs M_j = Ce [D2 : sym(Ce S_j)] + 2 sym(Ce S_j) T*;
+        // two columns per pass, so each row's Schmid vectors load once per pair
+        auto column_M = [&](int kj) {
             const M3 Sj = schmid_of(w.Sv + 6 * kj);
             const M3 Y = sym(mul(CE_tr, Sj));
             M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
             axpy(Mj, 2.0, mul(Y, Tst_tr));
+            return Mj;
+        };
+        int kj0 = 0;
+        for (; kj0 + 2 <= p_init; kj0 += 2) {
+            const M3 M0 = column_M(kj0), M1 = column_M(kj0 + 1);
+            const int b0 = w.pa0[kj0], b1 = w.pa0[kj0 + 1];
+            const unsigned long long n0 = (neg_d >> kj0) & 1ull, n1 = (neg_d >> (kj0 + 1)) & 1ull;
+            const double h0 = w.h[kj0], h1 = w.h[kj0 + 1];
+            for (int ki = 0; ki < p_init; ++ki) {
+                const int asys = w.pa0[ki];
+                double sv[6];
+#pragma unroll
+                for (int e = 0; e < 6; ++e) sv[e] = w.Sv[6 * ki + e];
+                const unsigned long long ni = (neg_d >> ki) & 1ull;
+                const double kin = w.kin[ki];
+                const double sm0 = schmid_dot(sv, M0), sm1 = schmid_dot(sv, M1);
+                double v0 = ldg(&L.q[asys * NM + b0]) * h0;
+                double v1 = ldg(&L.q[asys * NM + b1]) * h1;
+                v0 += (ni ^ n0) ? -sm0 : sm0;
+                v1 += (ni ^ n1) ? -sm1 : sm1;
+                v0 += kin;
+                v1 += kin;
+                w.A[ki * p_init + kj0] = v0;
+                w.A[ki * p_init + kj0 + 1] = v1;
+            }
+        }
+        for (int kj = kj0; kj < p_init; ++kj) {
+            const int bsys = w.pa0[kj];
+            const M3 Mj = column_M(kj);
             const unsigned long long nj = (neg_d >> kj) & 1ull;
             const double hj = w.h[kj];
             for (int ki = 0; ki < p_init; ++ki) {
