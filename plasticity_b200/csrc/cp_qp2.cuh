@@ -31,7 +31,7 @@ struct Scratch2 {
     unsigned char *pa0, *cur, *pos;
     double *tau_tr, *b, *h, *x_old, *x, *tn, *kin;
     double* Sv;   // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n (6 per k)
-    double* A;    // consistency matrix, leading dimension p_init
+    double* A;    // S_PA of the tangent, 9 rows of leading dimension PMAX
     double* Apa;  // the matrix being solved, leading dimension PMAX
     double* rhs;  // right-hand sides, 9 per row
 };
@@ -127,14 +127,65 @@ __host__ __device__ __forceinline__ void row_swap(double* a, double* b, int m) {
     }
 }
 
+// Two elimination steps j, j+1 on rows i0..i0+3 (row stride ld), columns
+// [c0, m): a_i[c] = (a_i[c] - f_i p[c]) - g_i q[c], with p, q the pivot rows
+// of steps j and j+1.  Each element sees the two subtractions of the
+// one-step-at-a-time elimination in the same order, but is loaded and stored
+// once for both.
+__host__ __device__ __forceinline__ void rows4_axpy2(double* a, int ld, const double* p, const double* q,
+                                                    const double f[4], const double g[4], int c0, int m) {
+    double* a0 = a;
+    double* a1 = a + ld;
+    double* a2 = a + 2 * ld;
+    double* a3 = a + 3 * ld;
+    int c = c0;
+    for (; c + 2 <= m; c += 2) {
+        double x[2], z[2], y0[2], y1[2], y2[2], y3[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            x[u] = p[c + u];
+            z[u] = q[c + u];
+            y0[u] = a0[c + u];
+            y1[u] = a1[c + u];
+            y2[u] = a2[c + u];
+            y3[u] = a3[c + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            a0[c + u] = (y0[u] - f[0] * x[u]) - g[0] * z[u];
+            a1[c + u] = (y1[u] - f[1] * x[u]) - g[1] * z[u];
+            a2[c + u] = (y2[u] - f[2] * x[u]) - g[2] * z[u];
+            a3[c + u] = (y3[u] - f[3] * x[u]) - g[3] * z[u];
+        }
+    }
+    for (; c < m; ++c) {
+        const double x = p[c], z = q[c];
+        const double y0 = a0[c], y1 = a1[c], y2 = a2[c], y3 = a3[c];
+        a0[c] = (y0 - f[0] * x) - g[0] * z;
+        a1[c] = (y1 - f[1] * x) - g[1] * z;
+        a2[c] = (y2 - f[2] * x) - g[2] * z;
+        a3[c] = (y3 - f[3] * x) - g[3] * z;
+    }
+}
+
 // lu_solve (cp_qp.cuh) with the batched row operations above and NRHS known
 // at compile time: Gaussian elimination with partial pivoting on the rows,
 // same pivots and same arithmetic per element, so the same results.
-template <int NRHS>
+//
+// With PAIR, steps are taken two at a time where both pivots are non-zero
+// (worth it for the larger solves only): column j+1 and row j+1 receive step
+// j's update first so that pivot j+1 is chosen on the same values, and the
+// rest of the trailing matrix then takes both updates in one pass.  Step j's
+// multiplier of row i is recomputed as a_i[j] times the pivot's reciprocal
+// wherever it is used (the same product each time).  A row swap of step j+1 before step j's update
+// of the columns right of j+1 changes nothing: that update of a row uses only
+// the row itself (its column j included, swapped with it) and pivot row j.
+template <int NRHS, bool PAIR>
 __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, double* B, double* cond = nullptr) {
     int sing = 0;
     double pmin = 1e308, pmax = 0.0;
-    for (int j = 0; j < m; ++j) {
+    // pivot search of step j and its row swap; false for a zero column
+    auto pivot = [&](int j) -> bool {
         int r = j;
         double mx = fabs(A[j * ld + j]);
         for (int i = j + 1; i < m; ++i) {
@@ -148,7 +199,7 @@ __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, dou
         pmax = fmax(pmax, mx);
         if (mx == 0.0) {
             sing = 1;
-            continue;
+            return false;
         }
         if (r != j) {
             row_swap(A + j * ld, A + r * ld, m);
@@ -159,18 +210,17 @@ __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, dou
                 B[r * NRHS + c] = t;
             }
         }
-        const double piv = 1.0 / A[j * ld + j];
-        double bj[NRHS];
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) bj[c] = B[j * NRHS + c];
-        int i = j + 1;
-        // four rows per pass (a zero multiplier leaves its row's finite
-        // entries unchanged, as skipping it would)
+        return true;
+    };
+    // step j alone on rows [i, m), columns [c0, m), pivot reciprocal piv (a
+    // zero multiplier leaves its row's finite entries unchanged, as skipping
+    // it would)
+    auto step1 = [&](int j, double piv, int i, int c0, const double* bj) {
         for (; i + 4 <= m; i += 4) {
             double f[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) f[r] = A[(i + r) * ld + j] * piv;
-            rows4_axpy(A + i * ld, ld, A + j * ld, f, j + 1, m);
+            rows4_axpy(A + i * ld, ld, A + j * ld, f, c0, m);
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -179,10 +229,73 @@ __host__ __device__ __forceinline__ int lu_solve_b(double* A, int m, int ld, dou
         for (; i < m; ++i) {
             const double f = A[i * ld + j] * piv;
             if (f == 0.0) continue;
-            row_axpy(A + i * ld, A + j * ld, f, j + 1, m);
+            row_axpy(A + i * ld, A + j * ld, f, c0, m);
 #pragma unroll
             for (int c = 0; c < NRHS; ++c) B[i * NRHS + c] -= f * bj[c];
         }
+    };
+    int j = 0;
+    while (j < m) {
+        if (!pivot(j)) {
+            ++j;
+            continue;
+        }
+        const double piv = 1.0 / A[j * ld + j];
+        double bj[NRHS];
+#pragma unroll
+        for (int c = 0; c < NRHS; ++c) bj[c] = B[j * NRHS + c];
+        if (!PAIR || j + 1 == m) {
+            step1(j, piv, j + 1, j + 1, bj);
+            ++j;
+            continue;
+        }
+        // step j on column j+1, then the pivot of step j+1 on those values
+        {
+            const double u = A[j * ld + j + 1];
+            for (int i = j + 1; i < m; ++i) A[i * ld + j + 1] = A[i * ld + j + 1] - (A[i * ld + j] * piv) * u;
+        }
+        if (!pivot(j + 1)) {
+            step1(j, piv, j + 1, j + 2, bj);
+            j += 2;
+            continue;
+        }
+        // row j+1 takes the rest of step j; then both steps on the rows below
+        const double f1 = A[(j + 1) * ld + j] * piv;
+        if (f1 != 0.0) {
+            row_axpy(A + (j + 1) * ld, A + j * ld, f1, j + 2, m);
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) B[(j + 1) * NRHS + c] -= f1 * bj[c];
+        }
+        const double piv1 = 1.0 / A[(j + 1) * ld + j + 1];
+        double bj1[NRHS];
+#pragma unroll
+        for (int c = 0; c < NRHS; ++c) bj1[c] = B[(j + 1) * NRHS + c];
+        int i = j + 2;
+        for (; i + 4 <= m; i += 4) {
+            double f[4], g[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                f[r] = A[(i + r) * ld + j] * piv;
+                g[r] = A[(i + r) * ld + j + 1] * piv1;
+            }
+            rows4_axpy2(A + i * ld, ld, A + j * ld, A + (j + 1) * ld, f, g, j + 2, m);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c)
+                    B[(i + r) * NRHS + c] = (B[(i + r) * NRHS + c] - f[r] * bj[c]) - g[r] * bj1[c];
+        }
+        for (; i < m; ++i) {
+            const double f = A[i * ld + j] * piv;
+            const double g = A[i * ld + j + 1] * piv1;
+            double* ai = A + i * ld;
+            const double* p = A + j * ld;
+            const double* q = A + (j + 1) * ld;
+            for (int c = j + 2; c < m; ++c) ai[c] = (ai[c] - f * p[c]) - g * q[c];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) B[i * NRHS + c] = (B[i * NRHS + c] - f * bj[c]) - g * bj1[c];
+        }
+        j += 2;
     }
     for (int j = m - 1; j >= 0; --j) {
         const double d = A[j * ld + j];
@@ -286,9 +399,10 @@ template <int PMAX>
 __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDev& g, int64_t i, const M3& F, int flag,
                                    double F_e, double F_r, const QpOut& out, int32_t* stats_out, int lattice_id,
                                    double* d2_slot, int d2_stride) {
+    constexpr bool kPairLU = PMAX > 32;  // paired elimination steps for the BCC-sized solves
     unsigned char pa0_[PMAX], cur_[PMAX], pos_[PMAX];
     double tau_tr_[PMAX], b_[PMAX], h_[PMAX], x_old_[PMAX], x_[PMAX], tn_[PMAX], kin_[PMAX];
-    double Sv_[PMAX * 6], A_[PMAX * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
+    double Sv_[PMAX * 6], A_[9 * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
     const Scratch2 w{pa0_, cur_, pos_, tau_tr_, b_, h_, x_old_, x_, tn_, kin_, Sv_, A_, Apa_, rhs_};
     const int n = L.n, ns = L.ns, nw = L.nw;
     const int64_t cnt = g.count;
@@ -403,8 +517,11 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             if (ng) neg_d |= (1ull << k);
             w.kin[k] = ng ? -kin : kin;
         }
-        // column j of A needs M_j = Ce [D2 : sym(Ce S_j)] + 2 sym(Ce S_j) T*;
-        // two columns per pass, so each row's Schmid vectors load once per pair
+        // A[PA,PA] is not stored: each removal round builds the rows and
+        // columns of its current set straight into the matrix it solves
+        // (same expression per entry, so the same values as a stored A).
+        // Column j needs M_j = Ce [D2 : sym(Ce S_j)] + 2 sym(Ce S_j) T*; two
+        // columns per pass, so each row's Schmid vectors load once per pair.
         auto column_M = [&](int kj) {
             const M3 Sj = schmid_of(w.Sv + 6 * kj);
             const M3 Y = sym(mul(CE_tr, Sj));
@@ -412,44 +529,50 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             axpy(Mj, 2.0, mul(Y, Tst_tr));
             return Mj;
         };
-        int kj0 = 0;
-        for (; kj0 + 2 <= p_init; kj0 += 2) {
-            const M3 M0 = column_M(kj0), M1 = column_M(kj0 + 1);
-            const int b0 = w.pa0[kj0], b1 = w.pa0[kj0 + 1];
-            const unsigned long long n0 = (neg_d >> kj0) & 1ull, n1 = (neg_d >> (kj0 + 1)) & 1ull;
-            const double h0 = w.h[kj0], h1 = w.h[kj0 + 1];
-            for (int ki = 0; ki < p_init; ++ki) {
-                const int asys = w.pa0[ki];
-                double sv[6];
+        auto build_active = [&](int m) {
+            int c = 0;
+            for (; c + 2 <= m; c += 2) {
+                const int kj0 = w.pos[c], kj1 = w.pos[c + 1];
+                const M3 M0 = column_M(kj0), M1 = column_M(kj1);
+                const int b0 = w.pa0[kj0], b1 = w.pa0[kj1];
+                const unsigned long long n0 = (neg_d >> kj0) & 1ull, n1 = (neg_d >> kj1) & 1ull;
+                const double h0 = w.h[kj0], h1 = w.h[kj1];
+                for (int r = 0; r < m; ++r) {
+                    const int ki = w.pos[r];
+                    const int asys = w.pa0[ki];
+                    double sv[6];
 #pragma unroll
-                for (int e = 0; e < 6; ++e) sv[e] = w.Sv[6 * ki + e];
-                const unsigned long long ni = (neg_d >> ki) & 1ull;
-                const double kin = w.kin[ki];
-                const double sm0 = schmid_dot(sv, M0), sm1 = schmid_dot(sv, M1);
-                double v0 = ldg(&L.q[asys * NM + b0]) * h0;
-                double v1 = ldg(&L.q[asys * NM + b1]) * h1;
-                v0 += (ni ^ n0) ? -sm0 : sm0;
-                v1 += (ni ^ n1) ? -sm1 : sm1;
-                v0 += kin;
-                v1 += kin;
-                w.A[ki * p_init + kj0] = v0;
-                w.A[ki * p_init + kj0 + 1] = v1;
+                    for (int e = 0; e < 6; ++e) sv[e] = w.Sv[6 * ki + e];
+                    const unsigned long long ni = (neg_d >> ki) & 1ull;
+                    const double kin = w.kin[ki];
+                    const double sm0 = schmid_dot(sv, M0), sm1 = schmid_dot(sv, M1);
+                    double v0 = ldg(&L.q[asys * NM + b0]) * h0;
+                    double v1 = ldg(&L.q[asys * NM + b1]) * h1;
+                    v0 += (ni ^ n0) ? -sm0 : sm0;
+                    v1 += (ni ^ n1) ? -sm1 : sm1;
+                    v0 += kin;
+                    v1 += kin;
+                    w.Apa[r * PMAX + c] = v0;
+                    w.Apa[r * PMAX + c + 1] = v1;
+                }
             }
-        }
-        for (int kj = kj0; kj < p_init; ++kj) {
-            const int bsys = w.pa0[kj];
-            const M3 Mj = column_M(kj);
-            const unsigned long long nj = (neg_d >> kj) & 1ull;
-            const double hj = w.h[kj];
-            for (int ki = 0; ki < p_init; ++ki) {
-                const int asys = w.pa0[ki];
-                const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
-                double v = ldg(&L.q[asys * NM + bsys]) * hj;
-                v += (((neg_d >> ki) & 1ull) ^ nj) ? -sm : sm;
-                v += w.kin[ki];
-                w.A[ki * p_init + kj] = v;
+            for (; c < m; ++c) {
+                const int kj = w.pos[c];
+                const int bsys = w.pa0[kj];
+                const M3 Mj = column_M(kj);
+                const unsigned long long nj = (neg_d >> kj) & 1ull;
+                const double hj = w.h[kj];
+                for (int r = 0; r < m; ++r) {
+                    const int ki = w.pos[r];
+                    const int asys = w.pa0[ki];
+                    const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
+                    double v = ldg(&L.q[asys * NM + bsys]) * hj;
+                    v += (((neg_d >> ki) & 1ull) ^ nj) ? -sm : sm;
+                    v += w.kin[ki];
+                    w.Apa[r * PMAX + c] = v;
+                }
             }
-        }
+        };
 
         // ---- consistency iterations (:311-448)
         for (int k = 0; k < p_init; ++k) {
@@ -469,24 +592,10 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 int m = 0;
                 for (int k = 0; k < p_init; ++k)
                     if (w.cur[k]) w.pos[m++] = (unsigned char)k;
-                for (int r = 0; r < m; ++r) {
-                    const int kr = w.pos[r];
-                    w.rhs[r] = w.b[kr];
-                    const double* Ar = w.A + kr * p_init;
-                    double* Pr = w.Apa + r * PMAX;
-                    int c = 0;
-                    for (; c + 4 <= m; c += 4) {  // four gathers in flight per step
-                        const int c0 = w.pos[c], c1 = w.pos[c + 1], c2 = w.pos[c + 2], c3 = w.pos[c + 3];
-                        const double v0 = Ar[c0], v1 = Ar[c1], v2 = Ar[c2], v3 = Ar[c3];
-                        Pr[c] = v0;
-                        Pr[c + 1] = v1;
-                        Pr[c + 2] = v2;
-                        Pr[c + 3] = v3;
-                    }
-                    for (; c < m; ++c) Pr[c] = Ar[w.pos[c]];
-                }
+                for (int r = 0; r < m; ++r) w.rhs[r] = w.b[w.pos[r]];
+                build_active(m);
                 double cnd = 1.0;
-                if (lu_solve_b<1>(w.Apa, m, PMAX, w.rhs, &cnd)) status |= QP_SINGULAR;
+                if (lu_solve_b<1, kPairLU>(w.Apa, m, PMAX, w.rhs, &cnd)) status |= QP_SINGULAR;
                 maxcond = fmax(maxcond, cnd);
                 ++rounds_total;
                 for (int k = 0; k < p_init; ++k) w.x[k] = 0.0;
@@ -662,8 +771,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 c_terms = count3;
             }
             const M3 X6 = mul(CE_tr, matexp(scale(-1.0, del_FP), nullptr, &status));
-            // S_PA (9 x p, :734-796) lives in the consistency matrix's storage,
-            // which this pass no longer reads (PMAX^2 >= 9 PMAX >= 9 p)
+            // S_PA (9 x p, :734-796): 9 rows of stride PMAX
             double* SPA = w.A;
             for (int cj = 0; cj < p; ++cj) {
                 const int kj = w.pos[cj];
@@ -691,7 +799,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
 #pragma unroll
                 for (int c = 0; c < 9; ++c) SPA[c * PMAX + cj] = nj ? -spa.a[c] : spa.a[c];
             }
-            if (lu_solve_b<9>(w.Apa, p, PMAX, w.rhs)) status |= QP_SINGULAR;
+            if (lu_solve_b<9, kPairLU>(w.Apa, p, PMAX, w.rhs)) status |= QP_SINGULAR;
             if (o.max_search == 1) {  // this is the last pass: keep S_PA and delgamma
                 lazy_p = p;
                 ++iter1;

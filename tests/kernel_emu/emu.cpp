@@ -119,3 +119,34 @@ extern "C" int emu_update(const cp_material_t* mat, const cp_options_t* opt, con
     for (int64_t i = 0; i < n; ++i) st->twin_iter[i] = twin_i[i];
     return 0;
 }
+
+// The batched solve of the compact update (lu_solve_b, one or two
+// elimination steps per pass) against the plain one (lu_solve) on the same matrix: m x m with
+// row stride ld, nrhs 1 or 9.  Returns 1 when solutions, factors (upper
+// triangle), singular flags and pivot-ratio estimates are bit-identical; the
+// only latitude is the sign of an exact zero (the plain form skips rows whose
+// multiplier is zero, the batched one subtracts 0 * x) and NaN payloads.
+static bool same_bits(double a, double b) {
+    if (std::memcmp(&a, &b, sizeof a) == 0) return true;
+    return (a == 0.0 && b == 0.0) || (a != a && b != b);
+}
+extern "C" int emu_lu_compare(const double* A0, const double* B0, int m, int ld, int nrhs, int pair) {
+    std::vector<double> a1(A0, A0 + (size_t)m * ld), a2 = a1;
+    std::vector<double> b1(B0, B0 + (size_t)m * nrhs), b2 = b1;
+    double c1 = 0.0, c2 = 0.0;
+    const int s1 = lu_solve(a1.data(), m, ld, b1.data(), nrhs, nrhs, &c1);
+    int s2;
+    if (pair)
+        s2 = nrhs == 9 ? lu_solve_b<9, true>(a2.data(), m, ld, b2.data(), &c2)
+                       : lu_solve_b<1, true>(a2.data(), m, ld, b2.data(), &c2);
+    else
+        s2 = nrhs == 9 ? lu_solve_b<9, false>(a2.data(), m, ld, b2.data(), &c2)
+                       : lu_solve_b<1, false>(a2.data(), m, ld, b2.data(), &c2);
+    if (s1 != s2 || !same_bits(c1, c2)) return 0;
+    for (size_t k = 0; k < b1.size(); ++k)
+        if (!same_bits(b1[k], b2[k])) return 0;
+    for (int i = 0; i < m; ++i)
+        for (int c = i; c < m; ++c)
+            if (!same_bits(a1[(size_t)i * ld + c], a2[(size_t)i * ld + c])) return 0;
+    return 1;
+}

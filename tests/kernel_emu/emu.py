@@ -20,6 +20,7 @@ def lib():
         D, I32 = C.POINTER(C.c_double), C.POINTER(C.c_int32)
         L.emu_update.argtypes = [C.POINTER(CpMaterial), C.POINTER(CpOptions), C.POINTER(O.OrState), D, C.c_int32,
                                  C.c_double, C.c_double, D, D, D, I32, I32, C.c_int32]
+        L.emu_lu_compare.argtypes = [D, D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         _lib = L
     return _lib
 

@@ -64,3 +64,45 @@ def test_kernel_source_general_caps(oracle_lib, emu):
     assert ok.mean() > 0.95
     assert (ob.stats()[:, 5] > 2).any()  # more than one slip-search pass happened
     assert rel_err(Pe[ok], Po[ok]) < TOL and rel_err(De[ok], Do[ok]) < TOL
+
+
+def _lu_cases(rng):
+    """Dense, graded, rank-deficient, zero-column and zero-row matrices of the
+    sizes the removal solves and the tangent solve see (1..48)."""
+    for m in list(range(1, 13)) + [15, 16, 23, 31, 32, 47, 48]:
+        yield m, rng.standard_normal((m, m))
+        yield m, rng.standard_normal((m, m)) * np.logspace(0, 12, m)[None, :]
+        if m > 1:
+            A = rng.standard_normal((m, m))
+            A[:, rng.integers(m)] = 0.0  # zero column: flagged singular, step skipped
+            yield m, A
+            A = rng.standard_normal((m, m))
+            A[rng.integers(m)] = 0.0
+            yield m, A
+            A = rng.standard_normal((m, m))
+            A[:, -1] = A[:, 0]  # rank deficient: exact cancellation in the last pivot
+            yield m, A
+            A = rng.standard_normal((m, m))
+            A[:, 1] = 0.0  # the second step of a pair is the zero column
+            yield m, A
+        A = np.where(rng.random((m, m)) < 0.6, 0.0, rng.standard_normal((m, m)))  # sparse: zero multipliers
+        yield m, A
+
+
+@pytest.mark.parametrize("pair", [0, 1], ids=["one_step", "paired_steps"])
+@pytest.mark.parametrize("nrhs", [1, 9])
+def test_batched_lu_bit_identical_to_plain(emu, nrhs, pair):
+    import ctypes as C
+    rng = np.random.default_rng(11)
+    D = C.POINTER(C.c_double)
+    n = 0
+    for m, A in _lu_cases(rng):
+        ld = 48
+        Ap = np.zeros((m, ld))
+        Ap[:, :m] = A
+        Ap = np.ascontiguousarray(Ap)
+        B = np.ascontiguousarray(rng.standard_normal((m, nrhs)))
+        ok = emu.lib().emu_lu_compare(Ap.ctypes.data_as(D), B.ctypes.data_as(D), m, ld, nrhs, pair)
+        assert ok == 1, (m, nrhs, n)
+        n += 1
+    assert n > 100
