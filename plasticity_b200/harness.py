@@ -29,6 +29,8 @@ from __future__ import annotations
 
 import dataclasses
 
+import math
+
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
@@ -145,6 +147,106 @@ def dirichlet_increments(mesh: StructuredMesh, bc_table, n_increments: int):
     return dofs, vals
 
 
+def face_precedence(mesh: StructuredMesh, pairs):
+    """Constrained dof -> the (face, dof) entry that sets it: a node on several
+    constrained faces takes the lowest face id, as the early return in
+    setBoundaryValues does (boundaryConditions.cc:79-113, :148-246)."""
+    owner = {}
+    for face in range(1, 7):
+        for f, dof in sorted(set((int(f), int(d)) for f, d in pairs)):
+            if f != face:
+                continue
+            for nd in face_nodes(mesh, face):
+                owner.setdefault(3 * nd + (dof - 1), (f, dof))
+    dofs = np.array(sorted(owner), dtype=np.int64)
+    return dofs, [owner[d] for d in dofs]
+
+
+class CyclicLoading:
+    """Simple face BCs plus one cyclic (face, dof): its nodes move by
+    +-du_c per increment, du_c = U_total dt / t_quarter, positive while
+    fmod(k dt, 4 t_quarter) < t_quarter or >= 3 t_quarter, negative between
+    (boundaryConditions.cc:15-77; ellipticBVP/init.cc:326-346; cycle time
+    ellipticBVP.cc:39).  The cyclic dof is checked before the face table, so
+    its nodes take it whatever other face they lie on."""
+
+    def __init__(self, mesh, bc_table, n_increments, delT, face, dof, quarter):
+        self.k = 0
+        self.delT, self.quarter = float(delT), float(quarter)
+        total = {(int(f), int(d)): float(u) for f, d, u in bc_table}
+        cyc = set(3 * face_nodes(mesh, int(face)) + (int(dof) - 1))
+        base_dofs, base_vals = dirichlet_increments(mesh, bc_table, n_increments)
+        vals = {int(g): v for g, v in zip(base_dofs, base_vals)}
+        self.du_c = total.get((int(face), int(dof)), 0.0) / n_increments * n_increments * self.delT / self.quarter
+        self.dofs = np.array(sorted(set(vals) | cyc), dtype=np.int64)
+        self.is_cyc = np.array([g in cyc for g in self.dofs])
+        self.base = np.array([0.0 if g in cyc else vals[g] for g in self.dofs])
+
+    def next_values(self, mesh, dofs):
+        r = math.fmod(self.k * self.delT, 4 * self.quarter)
+        sign = 1.0 if r < self.quarter else (-1.0 if r < 3 * self.quarter else 1.0)
+        self.k += 1
+        return np.where(self.is_cyc, sign * self.du_c, self.base)
+
+
+class TabularLoading:
+    """Piecewise-linear face displacements: rows (face, dof, U at the times of
+    the time table); in increment k (time (k+1) dt) a constrained dof moves by
+    dt times the slope of its row on the current time interval, the interval
+    advancing once the time passes its end (boundaryConditions.cc:148-246;
+    ellipticBVP/init.cc:388-408)."""
+
+    def __init__(self, mesh, rows, times, delT):
+        self.rows = {(int(r[0]), int(r[1])): np.asarray(r[2:], float) for r in rows}
+        self.times = np.asarray(times, float)
+        self.delT = float(delT)
+        self.k = 0
+        self.tc = 1
+        self.dofs, owners = face_precedence(mesh, list(self.rows))
+        self.owners = owners
+
+    def next_values(self, mesh, dofs):
+        t = self.delT * (self.k + 1)
+        if self.k == 0:
+            self.tc = 1
+        while self.tc + 1 < len(self.times) and t > self.times[self.tc]:
+            self.tc += 1
+        self.k += 1
+        tc, T = self.tc, self.times
+        slope = {key: (u[tc] - u[tc - 1]) / (T[tc] - T[tc - 1]) * self.delT for key, u in self.rows.items()}
+        return np.array([slope[o] for o in self.owners])
+
+
+def boundary_dofs(mesh: StructuredMesh, eps: float = 1e-5):
+    """Every dof of every node on the cube's surface: the velocity-gradient
+    boundary condition sets all of them (setBoundaryValues,
+    boundaryConditions.cc:269-274, which applyDirichletBCs calls for each dof
+    of each boundary face, :453-497)."""
+    x = mesh.node_xyz
+    nodes = np.nonzero(((x <= eps) | (x >= 1.0 - eps)).any(axis=1))[0]
+    return (3 * nodes[:, None] + np.arange(3)[None, :]).ravel().astype(np.int64)
+
+
+class VelocityGradientLoading:
+    """Macroscopic velocity gradient L applied in steps dt: before increment k,
+    F_k = (I - L dt)^-1 F_{k-1} with F_0 = I (updateBeforeIncrement.cc:10-30,
+    ellipticBVP/init.cc:551), and the boundary node at X moves by
+    (F_k - F_{k-1}) X in the increment's first Newton pass
+    (boundaryConditions.cc:269-274)."""
+
+    def __init__(self, L, dt):
+        self.L = np.asarray(L, dtype=np.float64).reshape(3, 3)
+        self.dt = float(dt)
+        self.F = np.eye(3)
+
+    def next_values(self, mesh: StructuredMesh, dofs):
+        F_new = np.linalg.inv(np.eye(3) - self.L * self.dt) @ self.F
+        dF = F_new - self.F
+        self.F = F_new
+        X = mesh.node_xyz[dofs // 3]
+        return (X @ dF.T)[np.arange(len(dofs)), dofs % 3]
+
+
 def von_mises_rows(rows):
     """run_compile_tests.py:45-48 on stressstrain rows."""
     r = np.asarray(rows)
@@ -173,11 +275,15 @@ class NewtonHarness:
     """Fixed-iteration Newton loop over a structured Q1 mesh."""
 
     def __init__(self, backend, mesh: StructuredMesh, bc_table, n_increments: int, max_newton: int = 4,
-                 multiphase: bool = False, device_system: bool = False, solver=None):
+                 multiphase: bool = False, device_system: bool = False, solver=None, vel_grad=None, delT=None,
+                 cyclic=None, tabular=None):
         """device_system: run the global system on the GPU (cp_bind_dofs /
         cp_newton_iteration / cp_update_from_displacement) with 'solver'
         (capi.CpSolver, default BiCG 1e-10); otherwise assemble on the
-        backend and solve on the host with a sparse LU."""
+        backend and solve on the host with a sparse LU.  Boundary conditions:
+        bc_table (face, dof, total displacement), plus cyclic = (face, dof,
+        quarter-cycle time) for cyclic loading; or tabular = (rows, times);
+        or vel_grad (3x3); delT is the time step of the last three."""
         self.be = backend
         self.device_system = device_system
         self.solver = solver
@@ -186,7 +292,21 @@ class NewtonHarness:
         self.n_increments = n_increments
         self.max_newton = max_newton
         self.multiphase = multiphase
-        self.cdofs, self.cvals = dirichlet_increments(mesh, bc_table, n_increments)
+        if vel_grad is not None:
+            self.loading = VelocityGradientLoading(vel_grad, delT)
+            self.cdofs = boundary_dofs(mesh)
+            self.cvals = np.zeros(len(self.cdofs))
+        elif tabular is not None:
+            self.loading = TabularLoading(mesh, tabular[0], tabular[1], delT)
+            self.cdofs = self.loading.dofs
+            self.cvals = np.zeros(len(self.cdofs))
+        elif cyclic is not None:
+            self.loading = CyclicLoading(mesh, bc_table, n_increments, delT, *cyclic)
+            self.cdofs = self.loading.dofs
+            self.cvals = np.zeros(len(self.cdofs))
+        else:
+            self.loading = None
+            self.cdofs, self.cvals = dirichlet_increments(mesh, bc_table, n_increments)
         self.u = np.zeros(mesh.n_dofs)
         self.F_e = 0.0
         self.F_r = 0.0
@@ -218,6 +338,8 @@ class NewtonHarness:
     def step(self):
         """One increment: max_newton assemble+solve passes, then the commit."""
         mesh = self.mesh
+        if self.loading is not None:
+            self.cvals = self.loading.next_values(mesh, self.cdofs)
         if self.device_system:
             for it in range(self.max_newton):
                 self.solve_info.append(self.be.newton_iteration(self.cvals if it == 0 else None, self.F_e, self.F_r,
@@ -236,6 +358,9 @@ class NewtonHarness:
         avg = self.be.averages()
         self.be.reorient()
         self.be.commit()
+        # a multiphase run keeps F_r = F_e = F_s = 0, in the twin rule and in
+        # the output row (updateAfterIncrement.cc:718-725, :755)
+        twin_cols = [0.0, 0.0, 0.0] if self.multiphase else [avg[18], avg[19], avg[20]]
         if self.multiphase:
             self.F_e = self.F_r = 0.0
         else:
@@ -243,7 +368,7 @@ class NewtonHarness:
         E = avg[0:9].reshape(3, 3)
         T = avg[9:18].reshape(3, 3)
         row = [E[0, 0], E[1, 1], E[2, 2], E[1, 2], E[0, 2], E[0, 1],
-               T[0, 0], T[1, 1], T[2, 2], T[1, 2], T[0, 2], T[0, 1], avg[18], avg[19], avg[20]]
+               T[0, 0], T[1, 1], T[2, 2], T[1, 2], T[0, 2], T[0, 1]] + twin_cols
         self.rows.append(row)
         return row
 
@@ -261,12 +386,19 @@ def deck_setup(d, backend_factory, material_from_fixture, **harness_kw):
     tests/golden/kat_*.npz fixture's dict); harness_kw: NewtonHarness options
     such as device_system, solver."""
     mesh = StructuredMesh(tuple(int(x) for x in d["n_elem"]))
-    mat = material_from_fixture(d)
+    n_phases = 1 + sum(1 for k in d if k.startswith("ph") and k.endswith("_C6"))
+    mats = [material_from_fixture(d)] + [material_from_fixture(d, phase=k) for k in range(2, n_phases + 1)]
     n_inc = int(round(float(d["total_T"]) / float(d["delT"])))
-    be = backend_factory([mat], d)
+    be = backend_factory(mats, d)
     rod = np.repeat(d["cell_rodrigues"], 8, axis=0)
-    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
-    h = NewtonHarness(be, mesh, d["bc"], n_inc, int(d["max_newton"]), **harness_kw)
+    lid = np.repeat(np.asarray(d["cell_phase"], np.int32) - 1, 8) if "cell_phase" in d else \
+        np.zeros(mesh.n_cells * 8, np.int32)
+    be.bind_qps(lid, rod)
+    harness_kw.setdefault("multiphase", bool(int(d.get("multiphase", 0))))
+    tab = (d["tab_bc"], d["tab_times"]) if "tab_bc" in d else None
+    cyc = tuple(d["cyclic"]) if "cyclic" in d else None
+    h = NewtonHarness(be, mesh, d.get("bc"), n_inc, int(d["max_newton"]), vel_grad=d.get("vel_grad"),
+                      delT=float(d["delT"]), cyclic=cyc, tabular=tab, **harness_kw)
     return h, d
 
 

@@ -345,14 +345,25 @@ def random_rodrigues(rng: np.random.Generator, count: int):
     return q[:, 1:] / q0[:, None]
 
 
-def material_from_deck(d) -> CpMaterial:
+def material_from_deck(d, phase: int = 1) -> CpMaterial:
     """A material from a parsed reference input deck (the dict stored in
-    tests/golden/kat_*.npz: prm values plus slip/twin/q tables)."""
+    tests/golden/kat_*.npz: prm values plus slip/twin/q tables); phase k > 1
+    of a multiphase deck reads the keys stored under the prefix 'ph<k>_'."""
+    if phase > 1:
+        pre = f"ph{phase}_"
+        d = {k[len(pre):]: v for k, v in d.items() if k.startswith(pre)}
     kw = {}
     if int(d["twinning"]):
         kw = dict(twin_normals=d["twin_normals"], twin_dirs=d["twin_dirs"], twin_s0=d["twin_s0"],
                   twin_h0=d["twin_h0"], twin_s_s=d["twin_s_s"], twin_a=d["twin_a"],
                   q_full=d["q"], twin_threshold=float(d["twin_threshold"]),
                   twin_saturation=float(d["twin_saturation"]), twin_shear=float(d["twin_shear"]))
+    if "c1" in d:
+        # backstress constants of the slip systems, then of the twins (0 for the
+        # dummy twin of twinning off, userInputParameters.cc:303-311)
+        nw = len(d["twin_normals"]) if int(d["twinning"]) else 1
+        tw1 = d["c1_twin"] if "c1_twin" in d else np.zeros(nw)
+        tw2 = d["c2_twin"] if "c2_twin" in d else np.zeros(nw)
+        kw.update(c1=np.concatenate([d["c1"], tw1]), c2=np.concatenate([d["c2"], tw2]))
     return build_material(d["C6"], d["slip_normals"], d["slip_dirs"], d["q"], d["s0"], d["h0"],
                           d["s_s"], d["a"], **kw)

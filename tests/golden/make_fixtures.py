@@ -2,7 +2,7 @@
 reference's own input decks and golden stress-strain curves.
 
 Run in a container where the reference checkout exists:
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py /root/reference [case ...]
 
 For each case it stores what plasticity_b200.decks.load_deck reads from the
 deck (derived as the reference derives it):
@@ -12,7 +12,8 @@ deck (derived as the reference derives it):
   * the 8x8x8 mesh's per-cell Rodrigues vector: the grain of the voxel nearest
     to the cell centre, ties to the lower voxel (crystalOrientationsIO.cc:66-194,
     loadOrientations.cc:4-31), then the grain's row of orientations.txt;
-  * the BCinfo face/dof/total-displacement table (ellipticBVP/init.cc:326-343);
+  * the BCinfo face/dof/total-displacement table (ellipticBVP/init.cc:326-343),
+    or the velocity gradient of a velocity-gradient deck;
   * the golden rows tests/compile_tests/<case>/correct_stressstrain.txt and
     the number of rows run_compile_tests.py checks (599 or 999).
 """
@@ -32,13 +33,20 @@ CASES = {
     "bcc_simpleTension": "bcc/simpleTension",
     "hcp_simpleTension": "hcp/simpleTension",
     "hcp_compression": "hcp/compression",
+    "fcc_DeformationGraidientBCs": "fcc/DeformationGraidientBCs",
+    "fcc_tabularSimpleCompression": "fcc/tabularSimpleCompression",
+    "fcc_CyclicLoading": "fcc/CyclicLoading",
+    "fcc_RandomOrientationBlock": "fcc/FCC_RandomOrientationBlock",
+    "fcc_simpleCompression_Multiphase": "fcc/simpleCompression_Multiphase",
 }
 CHECK_ROWS = {"hcp_simpleTension": 599, "hcp_compression": 599}
 
 
-def main(ref_root):
+def main(ref_root, only=None):
     here = os.path.dirname(os.path.abspath(__file__))
     for name, sub in CASES.items():
+        if only and name not in only:
+            continue
         app = os.path.join(ref_root, "applications/crystalPlasticity", sub)
         d = load_deck(app, golden=os.path.join(ref_root, "tests/compile_tests", sub, "correct_stressstrain.txt"))
         for k in ("n_grains", "max_linear", "rel_linear_tol"):
@@ -50,4 +58,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:])

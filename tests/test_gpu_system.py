@@ -168,3 +168,24 @@ def test_device_newton_hcp_twinning_deck(cuda_lib):
     assert err["stress"] < 1e-3 and err["strain"] < 1e-3, err
     hh.be.close()
     hd.be.close()
+
+
+@pytest.mark.parametrize("case", ["fcc_DeformationGraidientBCs", "fcc_tabularSimpleCompression",
+                                  "fcc_CyclicLoading", "fcc_RandomOrientationBlock"])
+def test_device_newton_loading_modes(cuda_lib, case):
+    """The velocity-gradient (every boundary dof moves each increment),
+    tabular, cyclic-with-backstress and 5x8x10-block decks through the device
+    loop: same rows as the host-solve loop and within 2e-3 of the golden curve
+    over the first increments."""
+    n_inc = 12
+    fx = f"tests/golden/kat_{case}.npz"
+    hh, d = H.kat_setup(fx, _gpu_factory, M.material_from_deck)
+    hd, _ = H.kat_setup(fx, _gpu_factory, M.material_from_deck, device_system=True)
+    rh = hh.run(n_inc)
+    rd = hd.run(n_inc)
+    assert all(i["converged"] for i in hd.solve_info)
+    assert rel_err(rd[:, :12], rh[:, :12]) < 1e-6
+    err = H.golden_errors(rd, d["golden"], n_inc)
+    assert err["stress"] < 2e-3 and err["strain"] < 2e-3, err
+    hh.be.close()
+    hd.be.close()

@@ -13,7 +13,10 @@ from plasticity_b200.capi import default_options
 
 def _run(oracle_lib, case, n_inc):
     def factory(mats, d):
-        return oracle_lib.OracleBackend(mats, default_options(stress_tolerance=float(d["tol"])), nthreads=0)
+        opts = default_options(stress_tolerance=float(d["tol"]),
+                               max_slip_search_iterations=int(d["max_slip_search"]),
+                               max_solver_iterations=int(d["max_solver"]))
+        return oracle_lib.OracleBackend(mats, opts, nthreads=0)
 
     h, d = H.kat_setup(f"tests/golden/kat_{case}.npz", factory, M.material_from_deck)
     rows = h.run(n_inc)
@@ -40,9 +43,25 @@ def test_golden_curve_hcp_twin_prefix(oracle_lib):
     assert err["stress"] < 1e-2 and err["strain"] < 1e-2 and err["slip"] < 1e-2, err
 
 
+@pytest.mark.parametrize("case", ["fcc_DeformationGraidientBCs", "fcc_tabularSimpleCompression",
+                                  "fcc_CyclicLoading", "fcc_RandomOrientationBlock"])
+def test_golden_curve_prefix_loading_modes(oracle_lib, case):
+    """The other loading modes and meshes of the reference's compile tests:
+    the velocity-gradient boundary condition on the whole surface, tabular
+    (piecewise-linear in time) face displacements, cyclic loading with
+    kinematic hardening (backstress), and a 5x8x10 block of one grain per
+    element.  The first 30 increments reach plastic flow in every case."""
+    rows, d = _run(oracle_lib, case, 30)
+    err = H.golden_errors(rows, d["golden"], 30)
+    assert err["stress"] < 2e-3 and err["strain"] < 2e-3 and err["slip"] < 1e-2, err
+    assert rows[-1, 14] > 0
+
+
 @pytest.mark.slow
 @pytest.mark.parametrize("case", ["fcc_simpleTension", "bcc_simpleTension", "hcp_simpleTension",
-                                  "hcp_compression", "fcc_compression"])
+                                  "hcp_compression", "fcc_compression", "fcc_DeformationGraidientBCs",
+                                  "fcc_tabularSimpleCompression", "fcc_CyclicLoading",
+                                  "fcc_RandomOrientationBlock"])
 def test_golden_curve_full(oracle_lib, case):
     d = np.load(f"tests/golden/kat_{case}.npz")
     n = int(d["check_rows"]) + 1
