@@ -753,6 +753,41 @@ def rve_dualphase_leg(args, device, increments=40):
     return out
 
 
+def serve_leg(args, device, n_requests=24, rates=(4.0, 16.0, 64.0), slots=8):
+    """The served RVE stream, sampled: n_requests independent RVE solves per
+    arrival rate (Poisson), edge 8/12/16 elements, FCC/BCC/HCP (the batched
+    workload's lattices), 8-64 Voronoi grains, 10-20 increments of a random
+    traceless velocity gradient of norm 1e-3/s (dt = 1 s); admitted by a
+    device-memory budget (80 % of the free memory) with up to ``slots`` in
+    flight.  Against the same requests served one at a time.  Reports
+    solves/s and p50/p95/p99 latency (completion minus arrival)."""
+    import torch
+    from plasticity_b200 import serving as S
+    mats = materials()
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = int(0.8 * free)
+    out = {"workload": f"{n_requests} RVE requests per rate: edge 8/12/16, FCC/BCC/HCP, 8-64 grains, "
+                       "10-20 increments of a random traceless velocity gradient (norm 1e-3/s)",
+           "slots": slots, "budget_gb": budget / 1e9}
+    warm = S.request_stream(2, 0.0, 99, edges=(8,), increments=(2, 2))
+    S.RveServer(mats, budget, slots).run(warm)
+    base = S.request_stream(n_requests, 0.0, 6, edges=(8, 12, 16), increments=(10, 20))
+    t0 = time.perf_counter()
+    seq = S.RveServer(mats, budget, 1).run(base)
+    out["sequential"] = S.summarize(seq, time.perf_counter() - t0)
+    for rate in rates:
+        reqs = S.request_stream(n_requests, rate, 6, edges=(8, 12, 16), increments=(10, 20))
+        srv = S.RveServer(mats, budget, slots)
+        t0 = time.perf_counter()
+        res = srv.run(reqs)
+        summ = S.summarize(res, time.perf_counter() - t0)
+        summ["max_in_flight"] = srv.max_in_flight
+        summ["same_rows_as_sequential"] = bool(all(np.array_equal(a.rows, b.rows) for a, b in zip(seq, res)
+                                                   if a.rows is not None and b.rows is not None))
+        out[f"rate_{rate:g}"] = summ
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -767,6 +802,7 @@ def main():
     ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
     ap.add_argument("--rve-large", action="store_true", help="only time the 48^3 RVE's first increments")
+    ap.add_argument("--serve", action="store_true", help="only time the served RVE stream")
     ap.add_argument("--rve-dualphase", action="store_true",
                     help="only time the 32^3 BCC/HCP velocity-gradient RVE's first increments")
     args = ap.parse_args()
@@ -776,6 +812,9 @@ def main():
         return reference_arm(args)
     if args.rve_large:
         print(json.dumps({"rve_large": rve_large_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        return 0
+    if args.serve:
+        print(json.dumps({"serve": serve_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
         return 0
     if args.rve_dualphase:
         print(json.dumps({"rve_dualphase": rve_dualphase_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}),

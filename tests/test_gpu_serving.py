@@ -1,0 +1,27 @@
+"""The served RVE stream on the GPU: requests of different sizes and
+lattices solved concurrently (one handle and stream each) give the same
+stress-strain rows as each solved alone."""
+import numpy as np
+import pytest
+
+from plasticity_b200 import materials as M
+from plasticity_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+
+
+def test_results_identical_alone_and_in_the_mix(cuda_lib):
+    mats = [M.fcc_cu(), M.bcc_48(), M.hcp_mg()]
+    reqs = S.request_stream(5, rate=0.0, seed=9, edges=(4, 5, 6), grains=(4, 12), increments=(3, 4),
+                            norm=2e-3)
+    assert len({r.lattice for r in reqs}) > 1 and len({r.edge for r in reqs}) > 1
+    alone = S.RveServer(mats, budget_bytes=1 << 36, max_slots=1).run(reqs)
+    srv = S.RveServer(mats, budget_bytes=1 << 36, max_slots=5)
+    mixed = srv.run(reqs)
+    assert srv.max_in_flight > 1
+    for a, b in zip(alone, mixed):
+        assert a.error is None and b.error is None, (a.error, b.error)
+        assert a.converged and b.converged
+        assert a.rows.shape == (reqs[a.rid].n_increments, 15)
+        assert np.array_equal(a.rows, b.rows)
+    assert any(np.abs(r.rows[-1, 14]) > 0 for r in mixed)  # plastic slip in the mix
