@@ -803,6 +803,8 @@ def main():
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
     ap.add_argument("--rve-large", action="store_true", help="only time the 48^3 RVE's first increments")
     ap.add_argument("--serve", action="store_true", help="only time the served RVE stream")
+    ap.add_argument("--rve-increments", type=int, default=40,
+                    help="increments the dual-phase RVE leg times (of its 40)")
     ap.add_argument("--rve-dualphase", action="store_true",
                     help="only time the 32^3 BCC/HCP velocity-gradient RVE's first increments")
     args = ap.parse_args()
@@ -817,8 +819,8 @@ def main():
         print(json.dumps({"serve": serve_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
         return 0
     if args.rve_dualphase:
-        print(json.dumps({"rve_dualphase": rve_dualphase_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}),
-              flush=True)
+        print(json.dumps({"rve_dualphase": rve_dualphase_leg(args, int(os.environ.get("LOCAL_RANK", "0")),
+                                                             args.rve_increments)}), flush=True)
         return 0
     return ours(args)
 

@@ -322,6 +322,7 @@ struct cp_handle {
         unsigned char* d_cmask = nullptr;       // n_dofs
         double *d_vals = nullptr, *d_Ke = nullptr, *d_Re = nullptr, *d_Ul = nullptr, *d_duc = nullptr;
         double* d_valsT = nullptr;              // K^T's values in K's pattern (per solve)
+        bool triples = false;                   // rows 3t..3t+2 share one column pattern
         int64_t n_blocks = 0;                   // node blocks (0: unavailable)
         int64_t *d_blk = nullptr, *d_blkpos = nullptr;  // 3 dofs / 9 entry positions per node block
         double* d_binv = nullptr;               // inverted 3x3 blocks (per solve)
@@ -1340,6 +1341,14 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
         rp[i + 1] = (int64_t)col.size();
     }
     const int64_t nnz = (int64_t)col.size();
+    // the three dofs of a node (3t, 3t+1, 3t+2) with one column pattern
+    bool triples = n_dofs % 3 == 0;
+    for (int64_t t = 0; triples && t < n_dofs / 3; ++t) {
+        const int64_t a = rp[3 * t], len = rp[3 * t + 1] - a;
+        triples = rp[3 * t + 2] - rp[3 * t + 1] == len && rp[3 * t + 3] - rp[3 * t + 2] == len;
+        for (int64_t j = 0; triples && j < len; ++j)
+            triples = col[a + j] == col[a + len + j] && col[a + j] == col[a + 2 * len + j];
+    }
     auto find = [&](int64_t i, int j) -> int64_t {
         const auto b = col.begin() + rp[i], e = col.begin() + rp[i + 1];
         return (int64_t)(std::lower_bound(b, e, j) - col.begin());
@@ -1407,6 +1416,7 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
     y.nnz = nnz;
     y.n_con = n_constrained;
     y.n_blocks = n_blocks;
+    y.triples = triples;
     if (n_blocks &&
         (cudaMalloc(&y.d_blk, sizeof(int64_t) * 3 * n_blocks) != cudaSuccess ||
          cudaMalloc(&y.d_blkpos, sizeof(int64_t) * 9 * n_blocks) != cudaSuccess ||
@@ -1533,9 +1543,15 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
                                                                       done);
         fbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
                                                               s.d_done, s.d_info);
-        fbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
-            s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_P), v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
-            s.d_ticket + 1, done);
+        if (s.triples)  // a warp per node, grid of 148 x 8 blocks at most (<= n / 8 partials)
+            fbicg_spmv3_kernel<<<(int)std::min<int64_t>(blocks_for(32 * (n / 3), SOLVE_BLOCK), SPMV3_GRID),
+                                 SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_P),
+                                                              v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
+                                                              s.d_ticket + 1, done);
+        else
+            fbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+                s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_P), v(V_PT), n, v(V_Q), v(V_QT), s.d_sc,
+                s.d_fpartial, s.d_ticket + 1, done);
         fbicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_P), v(V_Q), v(V_QT), v(V_DINV), n,
                                                                sv.rel_tolerance, sv.precond_norm, v(V_X), v(V_RES),
                                                                v(V_RT), s.d_fpartial, s.d_ticket + 2, s.d_done,

@@ -18,6 +18,7 @@
 namespace cp {
 
 constexpr int SOLVE_BLOCK = 256;
+constexpr int SPMV3_GRID = 148 * 8;  // node-triple SpMV: 8 resident 256-thread blocks per SM
 constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs
 
 // ---- gather / scatter ----------------------------------------------------
@@ -414,6 +415,59 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv_kernel(
             q[row] = s;
             qt[row] = st;
             v = pt[row] * s;
+        }
+    }
+    last_block_sum(v, partial, ticket, sc + SC_DEN);
+}
+
+// (3, node triples) the same when the three rows of every node (dofs 3t,
+// 3t+1, 3t+2) share one column pattern, as a nodal vector field's stiffness
+// does: a warp per node (grid-stride), each column index and p[c], p~[c]
+// loaded once for the three rows.  Every row's sums run in the same order as
+// in the row kernel (lane j takes entries j, j+32, ... of the row, then the
+// same shuffle tree), so q and q~ are the same; den = p~ . q is summed node by
+// node in a grid of fixed size.
+__global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv3_kernel(
+    const int64_t* __restrict__ row_ptr, const int* __restrict__ col, const double* __restrict__ vals,
+    const double* __restrict__ valsT, const double* __restrict__ p, const double* __restrict__ pt, int64_t n,
+    double* __restrict__ q, double* __restrict__ qt, double* __restrict__ sc, double* __restrict__ partial,
+    unsigned int* __restrict__ ticket, const int* __restrict__ done) {
+    if (*done) return;
+    const int64_t nt = n / 3;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    double v = 0.0;
+    for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nt; t += nw) {
+        const int64_t k0 = row_ptr[3 * t];
+        const int64_t len = row_ptr[3 * t + 1] - k0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
+        for (int64_t j = lane; j < len; j += 32) {
+            const int c = col[k0 + j];
+            const double pc = p[c], tc = pt[c];
+            s0 += vals[k0 + j] * pc;
+            s1 += vals[k0 + len + j] * pc;
+            s2 += vals[k0 + 2 * len + j] * pc;
+            u0 += valsT[k0 + j] * tc;
+            u1 += valsT[k0 + len + j] * tc;
+            u2 += valsT[k0 + 2 * len + j] * tc;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            u0 += __shfl_xor_sync(0xffffffffu, u0, o);
+            u1 += __shfl_xor_sync(0xffffffffu, u1, o);
+            u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+        }
+        if (lane == 0) {
+            q[3 * t] = s0;
+            q[3 * t + 1] = s1;
+            q[3 * t + 2] = s2;
+            qt[3 * t] = u0;
+            qt[3 * t + 1] = u1;
+            qt[3 * t + 2] = u2;
+            v += pt[3 * t] * s0 + pt[3 * t + 1] * s1 + pt[3 * t + 2] * s2;
         }
     }
     last_block_sum(v, partial, ticket, sc + SC_DEN);
