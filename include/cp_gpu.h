@@ -285,8 +285,12 @@ typedef struct cp_solver_t {
     int32_t check_every;    /* iterations queued between host checks of convergence (0: 8) */
     int32_t precond;        /* CP_PRECOND_* (the node blocks need the three components of every
                                node among one cell's local dofs 3a..3a+2, as cp_bind_dofs takes them) */
-    int32_t reserved;
+    int32_t kernel_mode;    /* 0: Jacobi BiCG of at most CP_PERSISTENT_MAX_DOFS dofs runs as one
+                               cooperative launch that iterates to convergence, larger systems as
+                               four kernels per iteration; 1: always four kernels per iteration;
+                               2: one cooperative launch at any size */
 } cp_solver_t;
+#define CP_PERSISTENT_MAX_DOFS 131072
 typedef struct cp_solve_info_t {
     int32_t iterations; /* Krylov iterations to convergence (or the cap) */
     int32_t converged;  /* 1 if the tolerance was met */

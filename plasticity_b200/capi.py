@@ -94,7 +94,7 @@ class CpSolver(C.Structure):
         ("precond_norm", C.c_int32),
         ("check_every", C.c_int32),
         ("precond", C.c_int32),
-        ("reserved", C.c_int32),
+        ("kernel_mode", C.c_int32),
     ]
 
 

@@ -329,7 +329,8 @@ struct cp_handle {
         double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
         double *d_sc = nullptr, *d_partial = nullptr;
         double* d_fpartial = nullptr;           // per-block partials of the fused iteration (n_dofs / 8 + 64)
-        unsigned int* d_ticket = nullptr;       // arrival counters of the fused reductions (4)
+        unsigned int* d_ticket = nullptr;       // [0..3] arrival counters of the fused reductions,
+                                                // [4..6] the persistent solve's barrier and timeout flag
         int *d_done = nullptr, *d_info = nullptr;
         // a block of Krylov iterations captured as CUDA graphs (first block /
         // later blocks), for the solver settings they were captured with
@@ -1449,7 +1450,7 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
               cudaMalloc(&y.d_sc, sizeof(double) * SC_COUNT) == cudaSuccess &&
               cudaMalloc(&y.d_partial, sizeof(double) * RED_BLOCKS) == cudaSuccess &&
               cudaMalloc(&y.d_fpartial, sizeof(double) * (n_dofs / 8 + 64)) == cudaSuccess &&
-              cudaMalloc(&y.d_ticket, sizeof(unsigned int) * 4) == cudaSuccess &&
+              cudaMalloc(&y.d_ticket, sizeof(unsigned int) * 8) == cudaSuccess &&
               cudaMalloc(&y.d_done, sizeof(int)) == cudaSuccess && cudaMalloc(&y.d_info, sizeof(int) * 3) == cudaSuccess;
     if (!ok) {
         free_system(h);
@@ -1468,7 +1469,7 @@ int cp_bind_dofs(cp_handle* h, int64_t n_dofs, const int64_t* h_cell_dofs, int64
         CK(h, cudaMemcpy(y.d_con, h_constrained, sizeof(int64_t) * n_constrained, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(y.d_cmask, cmask.data(), n_dofs, cudaMemcpyHostToDevice));
     CK(h, cudaMemset(y.d_vec, 0, sizeof(double) * SYS_VECS * n_dofs));
-    CK(h, cudaMemset(y.d_ticket, 0, sizeof(unsigned int) * 4));
+    CK(h, cudaMemset(y.d_ticket, 0, sizeof(unsigned int) * 8));
     return CP_OK;
 }
 
@@ -1610,9 +1611,15 @@ int cp_solver_default(cp_solver_t* sv) {
     sv->precond_norm = 0;
     sv->check_every = 8;
     sv->precond = CP_PRECOND_JACOBI;
-    sv->reserved = 0;
+    sv->kernel_mode = 0;
     return CP_OK;
 }
+
+// SpMV units (nodes or rows) per block of the persistent solve's grid: one per
+// warp keeps the dependent column / vector loads of the SpMV short
+#ifndef CP_PBICG_UNITS_PER_BLOCK
+#define CP_PBICG_UNITS_PER_BLOCK 8
+#endif
 
 int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
                         const cp_solver_t* solver, cp_solve_info_t* info) {
@@ -1672,7 +1679,7 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     CK(h, cudaMemsetAsync(s.d_done, 0, sizeof(int), h->stream));
     CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
     CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
-    CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 4, h->stream));
+    CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 8, h->stream));
     sys_dot(h, v(V_RHS), v(V_RHS), SC_BB, nullptr);
     sys_dot(h, v(V_RHS), v(V_RHS), SC_RR, nullptr);
     if (sv.precond_norm) {
@@ -1684,8 +1691,38 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     CK(h, cudaStreamSynchronize(h->stream));
     int hinfo[3] = {0, 0, 0};
     const double bnorm = std::sqrt(sc0[SC_BB]);
+    // one cooperative launch for the whole Jacobi BiCG solve (small systems,
+    // or on request) where the device can run one
+    bool persistent = sv.kind == CP_SOLVER_BICG && sv.precond == CP_PRECOND_JACOBI && sv.kernel_mode != 1 &&
+                      (sv.kernel_mode == 2 || n <= CP_PERSISTENT_MAX_DOFS);
+    int p_grid = 0;
+    if (persistent && bnorm != 0.0) {
+        int dev = 0, nsm = 0, coop = 0, per_sm = 0;
+        CK(h, cudaGetDevice(&dev));
+        CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK(h, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pbicg_kernel, SOLVE_BLOCK, 0));
+        const int64_t units = s.triples ? n / 3 : n;  // nodes or rows, CP_PBICG_UNITS_PER_BLOCK per block
+        p_grid = (int)std::max<int64_t>(
+            1, std::min<int64_t>((int64_t)nsm * per_sm,
+                                 (units + CP_PBICG_UNITS_PER_BLOCK - 1) / CP_PBICG_UNITS_PER_BLOCK));
+        persistent = coop && per_sm > 0 && 3 * (int64_t)p_grid <= n / 8 + 64;  // partials fit the scratch
+    }
     if (bnorm == 0.0) {
         hinfo[1] = 1;  // du = 0 solves it
+    } else if (persistent) {
+        PbicgArgs pa{s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_DINV), n, s.triples ? 1 : 0,
+                     sv.precond_norm, sv.max_iterations, sv.rel_tolerance, bnorm, v(V_X), v(V_RES), v(V_RT),
+                     v(V_Z), v(V_ZT), v(V_P), v(V_PT), v(V_Q), v(V_QT), s.d_fpartial, s.d_ticket + 4, s.d_info,
+                     reinterpret_cast<int*>(s.d_ticket + 6), s.d_sc};
+        void* kargs[] = {&pa};
+        CK(h, cudaLaunchCooperativeKernel((const void*)pbicg_kernel, dim3(p_grid), dim3(SOLVE_BLOCK), kargs, 0,
+                                          h->stream));
+        unsigned tk[8];
+        CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof hinfo, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(tk, s.d_ticket, sizeof tk, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        if (tk[6]) return fail(h, CP_E_CUDA, "cp_newton_iteration: a grid barrier of the solve timed out");
     } else {
         const int every = sv.check_every > 0 ? sv.check_every : 8;
         const bool graphs = ensure_solve_graphs(h, sv, every);

@@ -473,6 +473,229 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv3_kernel(
     last_block_sum(v, partial, ticket, sc + SC_DEN);
 }
 
+// ---- the whole Jacobi BiCG solve in one cooperative launch -----------------
+//
+// For systems small enough that the four kernels of an iteration are bound by
+// launch latency and host polling: one launch (cudaLaunchCooperativeKernel,
+// so every block is resident) iterates to convergence, the iteration cap or a
+// breakdown.  Same recurrence as the four kernels above; the phases of an
+// iteration are separated by grid barriers, three per iteration:
+//   [A] z = r / d, z~ = r~ / d, rho = z . r~ (with [D]'s reduction after the
+//       first iteration);  [B] p = z + beta p, p~ = z~ + beta p~;
+//   [C] q = K p, q~ = K^T p~, den = p~ . q;  [D] x, r, r~ updates, ||r||^2.
+// A reduction writes one partial per block; after the barrier every block
+// sums all partials in the same fixed order, so all blocks hold the same
+// scalar and the result does not depend on timing.  Values another block
+// wrote in this launch (p, p~, q, q~, the partials) are read through L2
+// (ld.global.cg), never the non-coherent or L1 paths.
+//
+// The barrier is a counter and a generation word.  Its wait is bounded: after
+// PBICG_SPIN_LIMIT polls it raises err and returns, and every block leaves at
+// its next barrier once err is set, so no launch can wait forever.
+constexpr long long PBICG_SPIN_LIMIT = 1ll << 25;
+
+struct PbicgArgs {
+    const int64_t* row_ptr;
+    const int* col;
+    const double* vals;
+    const double* valsT;
+    const double* dinv;
+    int64_t n;
+    int triples;       // rows 3t..3t+2 share one column pattern
+    int precond_norm;  // test ||M^-1 r|| instead of ||r||
+    int max_iter;
+    double tol;
+    double bnorm;  // ||b||
+    double *x, *r, *rt, *z, *zt, *p, *pt, *q, *qt;
+    double* partial;   // 3 x gridDim.x: rho, den, ||r||^2
+    unsigned* bar;     // [0] arrivals, [1] generation
+    int* info;         // [0] iterations, [1] converged, [2] breakdown
+    int* err;          // barrier timeout
+    double* sc;        // final scalars (SC_RR / SC_ZZ)
+};
+
+__device__ __forceinline__ bool pbicg_barrier(unsigned* bar, int* err) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            bar[0] = 0u;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g) {
+                if (++spins > PBICG_SPIN_LIMIT || *(volatile int*)err) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int*)err == 0;
+}
+
+// sum of partial[0 .. gridDim.x) in a fixed order (the same in every block)
+__device__ __forceinline__ double pbicg_allsum(const double* partial) {
+    __shared__ double total;
+    double f = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) f += __ldcg(partial + b);
+    f = block_sum(f);
+    if (threadIdx.x == 0) total = f;
+    __syncthreads();
+    const double t = total;
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ void pbicg_put(double v, double* partial) {
+    const double s = block_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
+    const int64_t n = a.n;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = tid >> 5, nwarps = nthreads >> 5;
+    // one partial row per reduced quantity: a row is rewritten only after
+    // every block has passed the barrier that follows its last read
+    double* P0 = a.partial;                  // rho
+    double* P1 = a.partial + gridDim.x;      // den
+    double* P2 = a.partial + 2 * gridDim.x;  // ||r||^2 (or ||M^-1 r||^2)
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    // [A] of the first iteration
+    {
+        double v = 0.0;
+        for (int64_t i = tid; i < n; i += nthreads) {
+            const double zi = a.r[i] * a.dinv[i], zti = a.rt[i] * a.dinv[i];
+            a.z[i] = zi;
+            a.zt[i] = zti;
+            v += zi * a.rt[i];
+        }
+        pbicg_put(v, P0);
+    }
+    if (!pbicg_barrier(a.bar, a.err)) return;
+    double rho = pbicg_allsum(P0), rho_old = 1.0;
+    for (int k = 0; k < a.max_iter; ++k) {
+        if (rho == 0.0 || !isfinite(rho)) {
+            if (lead) a.info[2] = 1;
+            return;
+        }
+        // [B]
+        const double beta = k == 0 ? 0.0 : rho / rho_old;
+        for (int64_t i = tid; i < n; i += nthreads) {
+            a.p[i] = a.z[i] + beta * a.p[i];
+            a.pt[i] = a.zt[i] + beta * a.pt[i];
+        }
+        if (!pbicg_barrier(a.bar, a.err)) return;
+        // [C]
+        {
+            double v = 0.0;
+            if (a.triples) {
+                for (int64_t t = warp; t < n / 3; t += nwarps) {
+                    const int64_t k0 = a.row_ptr[3 * t];
+                    const int64_t len = a.row_ptr[3 * t + 1] - k0;
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
+                    for (int64_t j = lane; j < len; j += 32) {
+                        const int c = a.col[k0 + j];
+                        const double pc = __ldcg(a.p + c), tc = __ldcg(a.pt + c);
+                        s0 += a.vals[k0 + j] * pc;
+                        s1 += a.vals[k0 + len + j] * pc;
+                        s2 += a.vals[k0 + 2 * len + j] * pc;
+                        u0 += a.valsT[k0 + j] * tc;
+                        u1 += a.valsT[k0 + len + j] * tc;
+                        u2 += a.valsT[k0 + 2 * len + j] * tc;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                        u0 += __shfl_xor_sync(0xffffffffu, u0, o);
+                        u1 += __shfl_xor_sync(0xffffffffu, u1, o);
+                        u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+                    }
+                    if (lane == 0) {
+                        a.q[3 * t] = s0;
+                        a.q[3 * t + 1] = s1;
+                        a.q[3 * t + 2] = s2;
+                        a.qt[3 * t] = u0;
+                        a.qt[3 * t + 1] = u1;
+                        a.qt[3 * t + 2] = u2;
+                        v += __ldcg(a.pt + 3 * t) * s0 + __ldcg(a.pt + 3 * t + 1) * s1 +
+                             __ldcg(a.pt + 3 * t + 2) * s2;
+                    }
+                }
+            } else {
+                for (int64_t row = warp; row < n; row += nwarps) {
+                    double s = 0.0, st = 0.0;
+                    for (int64_t kk = a.row_ptr[row] + lane; kk < a.row_ptr[row + 1]; kk += 32) {
+                        const int c = a.col[kk];
+                        s += a.vals[kk] * __ldcg(a.p + c);
+                        st += a.valsT[kk] * __ldcg(a.pt + c);
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        s += __shfl_xor_sync(0xffffffffu, s, o);
+                        st += __shfl_xor_sync(0xffffffffu, st, o);
+                    }
+                    if (lane == 0) {
+                        a.q[row] = s;
+                        a.qt[row] = st;
+                        v += __ldcg(a.pt + row) * s;
+                    }
+                }
+            }
+            pbicg_put(v, P1);
+        }
+        if (!pbicg_barrier(a.bar, a.err)) return;
+        const double den = pbicg_allsum(P1);
+        if (den == 0.0 || !isfinite(den)) {
+            if (lead) a.info[2] = 1;
+            return;
+        }
+        // [D] and the next [A]
+        const double alpha = rho / den;
+        {
+            double vr = 0.0, vz = 0.0;
+            for (int64_t i = tid; i < n; i += nthreads) {
+                a.x[i] += alpha * a.p[i];
+                const double ri = a.r[i] - alpha * __ldcg(a.q + i);
+                const double rti = a.rt[i] - alpha * __ldcg(a.qt + i);
+                a.r[i] = ri;
+                a.rt[i] = rti;
+                const double zi = ri * a.dinv[i], zti = rti * a.dinv[i];
+                a.z[i] = zi;
+                a.zt[i] = zti;
+                vr += a.precond_norm ? zi * zi : ri * ri;
+                vz += zi * rti;
+            }
+            pbicg_put(vr, P2);
+            pbicg_put(vz, P0);
+        }
+        if (!pbicg_barrier(a.bar, a.err)) return;
+        const double rr = pbicg_allsum(P2);
+        rho_old = rho;
+        rho = pbicg_allsum(P0);
+        if (lead) {
+            a.info[0] = k + 1;
+            a.sc[a.precond_norm ? SC_ZZ : SC_RR] = rr;
+        }
+        if (sqrt(rr) <= a.tol * a.bnorm) {
+            if (lead) a.info[1] = 1;
+            return;
+        }
+    }
+}
+
 // (4) x += alpha p; r -= alpha q; r~ -= alpha q~ (alpha = rho / den);
 // ||r||^2 (and ||M^-1 r||^2), then the convergence test in the last block;
 // rho_old = rho for the next iteration

@@ -137,6 +137,46 @@ def test_node_triple_and_row_spmv_agree(cuda_lib):
     be.close()
 
 
+@pytest.mark.parametrize("precond_norm", [0, 1])
+def test_persistent_solve_matches_four_kernel_iteration(cuda_lib, precond_norm):
+    """The whole Jacobi BiCG solve as one cooperative launch (kernel_mode 0
+    for this small system, 2 forced) against four kernels per iteration
+    (kernel_mode 1), from the same state: same du to the solver tolerance,
+    iteration counts within a few (the reductions sum in another order), and
+    the same for the row SpMV of a renumbered system."""
+    mesh = H.StructuredMesh((4, 4, 4))
+    rng = np.random.default_rng(37)
+    rod = np.repeat(M.random_rodrigues(rng, mesh.n_cells), 8, axis=0)
+    bc = np.array([[1, 1, 0.0], [3, 2, 0.0], [5, 3, 0.0], [2, 1, 0.004]])
+    be = CpHandle([M.fcc_cu()])
+    be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+    h = H.NewtonHarness(be, mesh, bc, 8, 4, device_system=True)
+    h.run(2)
+    u0 = be.get_displacement()
+    perm = rng.permutation(mesh.n_dofs)
+    for renumber in (False, True):
+        if renumber:
+            be.bind_dofs(mesh.n_dofs, perm[mesh.cell_dofs], perm[h.cdofs])
+            start = np.empty_like(u0)
+            start[perm] = u0
+        else:
+            start = u0
+        out = {}
+        for mode in (1, 0, 2):
+            be.set_displacement(start)
+            info = be.newton_iteration(h.cvals, h.F_e, h.F_r,
+                                       default_solver(kernel_mode=mode, precond_norm=precond_norm))
+            du = be.get_displacement() - start
+            out[mode] = (info, du[perm] if renumber else du)
+            assert info["converged"] and not info["breakdown"], (mode, info)
+            assert info["residual_norm"] <= 1e-10 * info["rhs_norm"] * (1 + 1e-12)
+        ref = out[1][1]
+        for mode in (0, 2):
+            assert np.abs(out[mode][1] - ref).max() <= 1e-7 * np.abs(ref).max(), (mode, renumber)
+            assert abs(out[mode][0]["iterations"] - out[1][0]["iterations"]) <= 5
+    be.close()
+
+
 def test_device_newton_petsc_norm(cuda_lib):
     """The stopping test PETSc's BiCG applies (preconditioned residual
     ||M^-1 r|| <= 1e-10 ||b||).  With Jacobi, M^-1 scales the residual by the
