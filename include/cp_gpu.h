@@ -290,7 +290,7 @@ typedef struct cp_solver_t {
                                four kernels per iteration; 1: always four kernels per iteration;
                                2: one cooperative launch at any size */
 } cp_solver_t;
-#define CP_PERSISTENT_MAX_DOFS 131072
+#define CP_PERSISTENT_MAX_DOFS 49152
 typedef struct cp_solve_info_t {
     int32_t iterations; /* Krylov iterations to convergence (or the cap) */
     int32_t converged;  /* 1 if the tolerance was met */

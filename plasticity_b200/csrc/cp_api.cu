@@ -1702,9 +1702,12 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         CK(h, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         CK(h, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pbicg_kernel, SOLVE_BLOCK, 0));
-        const int64_t units = s.triples ? n / 3 : n;  // nodes or rows, CP_PBICG_UNITS_PER_BLOCK per block
+        // nodes or rows, CP_PBICG_UNITS_PER_BLOCK per block, at most one block
+        // per SM: the solves of other handles (concurrent requests) keep room
+        // to run beside it
+        const int64_t units = s.triples ? n / 3 : n;
         p_grid = (int)std::max<int64_t>(
-            1, std::min<int64_t>((int64_t)nsm * per_sm,
+            1, std::min<int64_t>(std::min<int64_t>((int64_t)nsm * per_sm, nsm),
                                  (units + CP_PBICG_UNITS_PER_BLOCK - 1) / CP_PBICG_UNITS_PER_BLOCK));
         persistent = coop && per_sm > 0 && 3 * (int64_t)p_grid <= n / 8 + 64;  // partials fit the scratch
     }
