@@ -803,6 +803,7 @@ def main():
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
     ap.add_argument("--rve-large", action="store_true", help="only time the 48^3 RVE's first increments")
     ap.add_argument("--serve", action="store_true", help="only time the served RVE stream")
+    ap.add_argument("--rve-only", action="store_true", help="only time the 8^3 RVE solve on the device")
     ap.add_argument("--rve-increments", type=int, default=40,
                     help="increments the dual-phase RVE leg times (of its 40)")
     ap.add_argument("--rve-dualphase", action="store_true",
@@ -814,6 +815,18 @@ def main():
         return reference_arm(args)
     if args.rve_large:
         print(json.dumps({"rve_large": rve_large_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        return 0
+    if args.rve_only:
+        from plasticity_b200.capi import CpHandle, default_options
+        from plasticity_b200 import materials as M
+        be = CpHandle([M.fcc_cu()], default_options(device=int(os.environ.get("LOCAL_RANK", "0"))))
+        rows, t, h = rve_run(be, True)
+        print(json.dumps({"rve_device": {"seconds": t, "rve_solves_per_s": 1.0 / t,
+                                         "final_stress_xx_mpa": float(rows[-1][6]),
+                                         "linear_iterations_mean": float(np.mean([i["iterations"]
+                                                                                  for i in h.solve_info]))}}),
+              flush=True)
+        be.close()
         return 0
     if args.serve:
         print(json.dumps({"serve": serve_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
