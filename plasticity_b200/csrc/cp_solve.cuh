@@ -490,9 +490,17 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv3_kernel(
 // (ld.global.cg), never the non-coherent or L1 paths.
 //
 // The barrier is a counter and a generation word.  Its wait is bounded: after
-// PBICG_SPIN_LIMIT polls it raises err and returns, and every block leaves at
-// its next barrier once err is set, so no launch can wait forever.
-constexpr long long PBICG_SPIN_LIMIT = 1ll << 25;
+// PBICG_WAIT_NS of the global timer (or PBICG_SPIN_LIMIT polls) it raises err
+// and returns, and every block leaves at its next barrier once err is set, so
+// no launch can wait forever.
+constexpr long long PBICG_SPIN_LIMIT = 1ll << 24;
+constexpr unsigned long long PBICG_WAIT_NS = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 struct PbicgArgs {
     const int64_t* row_ptr;
@@ -526,9 +534,10 @@ __device__ __forceinline__ bool pbicg_barrier(unsigned* bar, int* err) {
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
+            const unsigned long long t0 = global_ns();
             long long spins = 0;
             while (*gen == g) {
-                if (++spins > PBICG_SPIN_LIMIT || *(volatile int*)err) {
+                if (++spins > PBICG_SPIN_LIMIT || *(volatile int*)err || global_ns() - t0 > PBICG_WAIT_NS) {
                     atomicExch(err, 1);
                     break;
                 }
