@@ -1716,7 +1716,8 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
     } else if (persistent) {
         PbicgArgs pa{s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_DINV), n, s.triples ? 1 : 0,
                      sv.precond_norm, sv.max_iterations, sv.rel_tolerance, bnorm, v(V_X), v(V_RES), v(V_RT),
-                     v(V_Z), v(V_ZT), v(V_P), v(V_PT), v(V_Q), v(V_QT), s.d_fpartial, s.d_ticket + 4, s.d_info,
+                     v(V_Z), v(V_ZT), v(V_P), v(V_PT), v(V_Q), v(V_QT), v(V_S), v(V_T), s.d_fpartial,
+                     s.d_ticket + 4, s.d_info,
                      reinterpret_cast<int*>(s.d_ticket + 6), s.d_sc};
         void* kargs[] = {&pa};
         CK(h, cudaLaunchCooperativeKernel((const void*)pbicg_kernel, dim3(p_grid), dim3(SOLVE_BLOCK), kargs, 0,

@@ -479,14 +479,15 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_spmv3_kernel(
 // launch latency and host polling: one launch (cudaLaunchCooperativeKernel,
 // so every block is resident) iterates to convergence, the iteration cap or a
 // breakdown.  Same recurrence as the four kernels above; the phases of an
-// iteration are separated by grid barriers, three per iteration:
-//   [A] z = r / d, z~ = r~ / d, rho = z . r~ (with [D]'s reduction after the
-//       first iteration);  [B] p = z + beta p, p~ = z~ + beta p~;
-//   [C] q = K p, q~ = K^T p~, den = p~ . q;  [D] x, r, r~ updates, ||r||^2.
+// iteration are separated by grid barriers, two per iteration:
+//   [B+C] p = z + beta p, p~ = z~ + beta p~ (formed where the SpMV reads them,
+//         double-buffered), q = K p, q~ = K^T p~, den = p~ . q;
+//   [D] x, r, r~ updates, ||r||^2, and the next z = r / d, z~ = r~ / d,
+//       rho = z . r~ (the first iteration's rho before the loop).
 // A reduction writes one partial per block; after the barrier every block
 // sums all partials in the same fixed order, so all blocks hold the same
 // scalar and the result does not depend on timing.  Values another block
-// wrote in this launch (p, p~, q, q~, the partials) are read through L2
+// wrote in this launch (z, z~, p, p~, q, q~, the partials) are read through L2
 // (ld.global.cg), never the non-coherent or L1 paths.
 //
 // The barrier is a counter and a generation word.  Its wait is bounded: after
@@ -515,6 +516,7 @@ struct PbicgArgs {
     double tol;
     double bnorm;  // ||b||
     double *x, *r, *rt, *z, *zt, *p, *pt, *q, *qt;
+    double *p2, *pt2;  // second buffers of the direction pair
     double* partial;   // 3 x gridDim.x: rho, den, ||r||^2
     unsigned* bar;     // [0] arrivals, [1] generation
     int* info;         // [0] iterations, [1] converged, [2] breakdown
@@ -598,14 +600,20 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
             if (lead) a.info[2] = 1;
             return;
         }
-        // [B]
+        // [B+C] the directions p = z + beta p_old, p~ = z~ + beta p~_old are
+        // formed where the SpMV needs them (every warp for the columns it
+        // reads, the same expression as the four-kernel iteration's), so no
+        // barrier separates them from the SpMV; the owner of a row stores its
+        // p, p~ into the other buffer of the pair for [D] and the next
+        // iteration
         const double beta = k == 0 ? 0.0 : rho / rho_old;
-        for (int64_t i = tid; i < n; i += nthreads) {
-            a.p[i] = a.z[i] + beta * a.p[i];
-            a.pt[i] = a.zt[i] + beta * a.pt[i];
-        }
-        if (!pbicg_barrier(a.bar, a.err)) return;
-        // [C]
+        const double* po = (k & 1) ? a.p2 : a.p;
+        const double* pto = (k & 1) ? a.pt2 : a.pt;
+        double* pn = (k & 1) ? a.p : a.p2;
+        double* ptn = (k & 1) ? a.pt : a.pt2;
+        auto dir = [&](const double* zv, const double* old, int64_t c) {
+            return k == 0 ? __ldcg(zv + c) : __ldcg(zv + c) + beta * __ldcg(old + c);
+        };
         {
             double v = 0.0;
             if (a.triples) {
@@ -615,7 +623,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
                     double s0 = 0.0, s1 = 0.0, s2 = 0.0, u0 = 0.0, u1 = 0.0, u2 = 0.0;
                     for (int64_t j = lane; j < len; j += 32) {
                         const int c = a.col[k0 + j];
-                        const double pc = __ldcg(a.p + c), tc = __ldcg(a.pt + c);
+                        const double pc = dir(a.z, po, c), tc = dir(a.zt, pto, c);
                         s0 += a.vals[k0 + j] * pc;
                         s1 += a.vals[k0 + len + j] * pc;
                         s2 += a.vals[k0 + 2 * len + j] * pc;
@@ -633,14 +641,21 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
                         u2 += __shfl_xor_sync(0xffffffffu, u2, o);
                     }
                     if (lane == 0) {
+                        const double t0 = dir(a.zt, pto, 3 * t), t1 = dir(a.zt, pto, 3 * t + 1),
+                                     t2 = dir(a.zt, pto, 3 * t + 2);
+                        pn[3 * t] = dir(a.z, po, 3 * t);
+                        pn[3 * t + 1] = dir(a.z, po, 3 * t + 1);
+                        pn[3 * t + 2] = dir(a.z, po, 3 * t + 2);
+                        ptn[3 * t] = t0;
+                        ptn[3 * t + 1] = t1;
+                        ptn[3 * t + 2] = t2;
                         a.q[3 * t] = s0;
                         a.q[3 * t + 1] = s1;
                         a.q[3 * t + 2] = s2;
                         a.qt[3 * t] = u0;
                         a.qt[3 * t + 1] = u1;
                         a.qt[3 * t + 2] = u2;
-                        v += __ldcg(a.pt + 3 * t) * s0 + __ldcg(a.pt + 3 * t + 1) * s1 +
-                             __ldcg(a.pt + 3 * t + 2) * s2;
+                        v += t0 * s0 + t1 * s1 + t2 * s2;
                     }
                 }
             } else {
@@ -648,8 +663,8 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
                     double s = 0.0, st = 0.0;
                     for (int64_t kk = a.row_ptr[row] + lane; kk < a.row_ptr[row + 1]; kk += 32) {
                         const int c = a.col[kk];
-                        s += a.vals[kk] * __ldcg(a.p + c);
-                        st += a.valsT[kk] * __ldcg(a.pt + c);
+                        s += a.vals[kk] * dir(a.z, po, c);
+                        st += a.valsT[kk] * dir(a.zt, pto, c);
                     }
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) {
@@ -657,9 +672,12 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
                         st += __shfl_xor_sync(0xffffffffu, st, o);
                     }
                     if (lane == 0) {
+                        const double tr = dir(a.zt, pto, row);
+                        pn[row] = dir(a.z, po, row);
+                        ptn[row] = tr;
                         a.q[row] = s;
                         a.qt[row] = st;
-                        v += __ldcg(a.pt + row) * s;
+                        v += tr * s;
                     }
                 }
             }
@@ -676,7 +694,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
         {
             double vr = 0.0, vz = 0.0;
             for (int64_t i = tid; i < n; i += nthreads) {
-                a.x[i] += alpha * a.p[i];
+                a.x[i] += alpha * __ldcg(pn + i);
                 const double ri = a.r[i] - alpha * __ldcg(a.q + i);
                 const double rti = a.rt[i] - alpha * __ldcg(a.qt + i);
                 a.r[i] = ri;
