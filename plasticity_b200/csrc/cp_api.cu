@@ -541,9 +541,15 @@ void sort_group(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m) {
 template <int PMAX, class FSrc>
 void launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m, int flag, double F_e, double F_r,
                     double* P, double* T, double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
-    update2_kernel<PMAX, FSrc><<<blocks_for(m, update2_block(PMAX)), update2_block(PMAX), 0, h->stream>>>(
-        h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, h->d_stats,
-        kF, kT, g.lattice);
+    if (m <= UPDATE2_SPREAD_QPS)
+        update2_kernel<PMAX, FSrc, UPDATE2_SPREAD_BLOCK, update2_spread_min_blocks(PMAX)>
+            <<<blocks_for(m, UPDATE2_SPREAD_BLOCK), UPDATE2_SPREAD_BLOCK, 0, h->stream>>>(
+                h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
+                h->d_stats, kF, kT, g.lattice);
+    else
+        update2_kernel<PMAX, FSrc><<<blocks_for(m, update2_block(PMAX)), update2_block(PMAX), 0, h->stream>>>(
+            h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
+            h->d_stats, kF, kT, g.lattice);
 }
 
 // calculatePlasticity over internal qps [i0, i0 + m) of group gi (sort + update)
