@@ -570,6 +570,59 @@ __device__ __forceinline__ void pbicg_put(double v, double* partial) {
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// block_sum of two values with one pass through shared memory (the same
+// shuffle tree and warp order per value as block_sum)
+__device__ __forceinline__ void block_sum2(double v0, double v1, double& s0, double& s1) {
+    __shared__ double sh2[2][SOLVE_BLOCK / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh2[0][threadIdx.x >> 5] = v0;
+        sh2[1][threadIdx.x >> 5] = v1;
+    }
+    __syncthreads();
+    s0 = 0.0;
+    s1 = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < SOLVE_BLOCK / 32; ++w) {
+            s0 += sh2[0][w];
+            s1 += sh2[1][w];
+        }
+    __syncthreads();
+}
+
+// pbicg_put / pbicg_allsum for two partial rows at once
+__device__ __forceinline__ void pbicg_put2(double v0, double v1, double* partial0, double* partial1) {
+    double s0, s1;
+    block_sum2(v0, v1, s0, s1);
+    if (threadIdx.x == 0) {
+        partial0[blockIdx.x] = s0;
+        partial1[blockIdx.x] = s1;
+    }
+}
+__device__ __forceinline__ void pbicg_allsum2(const double* partial0, const double* partial1, double& t0,
+                                              double& t1) {
+    __shared__ double total2[2];
+    double f0 = 0.0, f1 = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        f0 += __ldcg(partial0 + b);
+        f1 += __ldcg(partial1 + b);
+    }
+    double s0, s1;
+    block_sum2(f0, f1, s0, s1);
+    if (threadIdx.x == 0) {
+        total2[0] = s0;
+        total2[1] = s1;
+    }
+    __syncthreads();
+    t0 = total2[0];
+    t1 = total2[1];
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
     const int64_t n = a.n;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -705,13 +758,12 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
                 vr += a.precond_norm ? zi * zi : ri * ri;
                 vz += zi * rti;
             }
-            pbicg_put(vr, P2);
-            pbicg_put(vz, P0);
+            pbicg_put2(vr, vz, P2, P0);
         }
         if (!pbicg_barrier(a.bar, a.err)) return;
-        const double rr = pbicg_allsum(P2);
+        double rr;
         rho_old = rho;
-        rho = pbicg_allsum(P0);
+        pbicg_allsum2(P2, P0, rr, rho);
         if (lead) {
             a.info[0] = k + 1;
             a.sc[a.precond_norm ? SC_ZZ : SC_RR] = rr;
