@@ -1642,6 +1642,7 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         return fail(h, CP_E_ARG, "cp_newton_iteration: bad solver settings");
     if (sv.precond != CP_PRECOND_JACOBI && sv.precond != CP_PRECOND_NODE_BLOCK)
         return fail(h, CP_E_ARG, "cp_newton_iteration: unknown preconditioner");
+    if (sv.kernel_mode < 0 || sv.kernel_mode > 2) return fail(h, CP_E_ARG, "cp_newton_iteration: bad kernel_mode");
     if (sv.precond == CP_PRECOND_NODE_BLOCK && (sv.kind != CP_SOLVER_BICG || sv.precond_norm))
         return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: node blocks need BiCG with the true-residual test");
     if (sv.precond == CP_PRECOND_NODE_BLOCK && !s.n_blocks)

@@ -106,6 +106,8 @@ def test_device_newton_iteration_solves_the_condensed_system(cuda_lib):
         be.newton_iteration(None, h.F_e, h.F_r, default_solver(kind=CP_SOLVER_BICGSTAB, precond=CP_PRECOND_NODE_BLOCK))
     with pytest.raises(CpError):
         be.newton_iteration(None, h.F_e, h.F_r, default_solver(precond=7))
+    with pytest.raises(CpError):
+        be.newton_iteration(None, h.F_e, h.F_r, default_solver(kernel_mode=3))
     be.close()
 
 
