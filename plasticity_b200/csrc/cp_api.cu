@@ -1550,7 +1550,7 @@ void krylov_iteration(cp_handle* h, const cp_solver_t& sv, bool first) {
                                                                       done);
         fbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, v(V_Z), v(V_ZT), n, first, v(V_P), v(V_PT),
                                                               s.d_done, s.d_info);
-        if (s.triples)  // a warp per node, grid of 148 x 8 blocks at most (<= n / 8 partials)
+        if (s.triples)  // a warp per node, grid of SPMV3_GRID blocks at most (<= n / 8 partials)
             fbicg_spmv3_kernel<<<(int)std::min<int64_t>(blocks_for(32 * (n / 3), SOLVE_BLOCK), SPMV3_GRID),
                                  SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_vals, s.d_valsT, v(V_P),
                                                               v(V_PT), n, v(V_Q), v(V_QT), s.d_sc, s.d_fpartial,
