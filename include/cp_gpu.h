@@ -99,8 +99,13 @@ typedef struct cp_options_t {
     int32_t max_solver_iterations;      /* modelMaxSolverIterations */
     int32_t enable_multiphase;          /* F_T rule, calculatePlasticity.cc:970-980 */
     int32_t device;                     /* CUDA device ordinal */
-    int32_t block_size;                 /* reserved (0) */
-    int32_t use_graphs;                 /* reserved (0) */
+    int32_t update_variant;             /* launch shape of the sorted update: 0 = each lattice group's
+                                           shape chosen by cp_autotune, or the default rule before any
+                                           tuning; k in 1..CP_UPDATE_VARIANTS forces shape k-1 */
+    int32_t use_graphs;                 /* 1 (cp_options_default): the launches of a cp_update_device,
+                                           cp_assemble_device or cp_update_from_displacement call are
+                                           captured once as a CUDA graph and replayed while the call's
+                                           pointers, scalars and launch shapes repeat; 0: stream launches */
     int32_t plain_kernel;               /* 1: one thread per qp in bind order with full-size per-thread
                                            scratch (the plain FP64 drop-in, kept as a baseline);
                                            0 (default): qps sorted by potentially-active-set size each
@@ -193,6 +198,24 @@ int cp_assemble(cp_handle* h, const double* h_U_local, double F_e, double F_r,
                 double* h_Ke, double* h_Re, int32_t* h_status);
 int cp_assemble_device(cp_handle* h, const double* d_U_local, double F_e,
                        double F_r, double* d_Ke, double* d_Re, int32_t* d_status);
+
+/*
+ * Mixed-precision batched getElementalValues: the same sorted FP64 update
+ * (F gather, calculatePlasticity with the tangent), then the element
+ * contraction Ke = sum_q B^T (JxW dP/dF) B on the tensor cores in split-BF16
+ * (three bf16 terms per operand, six products) with FP32 accumulation:
+ * Ke is FP32 (576 per cell, relative error ~1e-7 of the cell's largest
+ * entry against the FP64 contraction), Re stays FP64 and equals
+ * cp_assemble's bit for bit (getElementalValues.cc:144-162).  Needs a
+ * uniform mesh (cp_bind_mesh uniform != 0) and the sorted update.  The
+ * device form is asynchronous: an expired wait inside the contraction
+ * (an error flag, no GPU fault) is reported by the next cp_synchronize;
+ * the host form reports it itself.
+ */
+int cp_assemble_mixed(cp_handle* h, const double* h_U_local, double F_e, double F_r,
+                      float* h_Ke, double* h_Re, int32_t* h_status);
+int cp_assemble_mixed_device(cp_handle* h, const double* d_U_local, double F_e,
+                             double F_r, float* d_Ke, double* d_Re, int32_t* d_status);
 
 /*
  * Volume averages over the bound mesh after a post-pass update, as
@@ -289,13 +312,25 @@ typedef struct cp_solver_t {
                                cooperative launch that iterates to convergence, larger systems as
                                four kernels per iteration; 1: always four kernels per iteration;
                                2: one cooperative launch at any size */
+    int32_t precision;      /* CP_PRECISION_FP64 (default): FP64 assembly and solve.
+                               CP_PRECISION_MIXED: the element contraction on the tensor cores
+                               (cp_assemble_mixed: FP32 Ke, FP64 Re), K scattered to FP32, and the
+                               solve as FP64 iterative refinement (r = b - K x in FP64 products of
+                               K's FP32 values, stopped at ||r|| <= rel_tolerance ||b||) around
+                               FP32 Jacobi BiCG inner solves to a relative residual of 1e-5
+                               (max_iterations each); BiCG + Jacobi and the true-residual test
+                               only; needs a uniform mesh */
+    int32_t max_refinements; /* CP_PRECISION_MIXED: outer refinement passes (0: 10) */
 } cp_solver_t;
+#define CP_PRECISION_FP64 0
+#define CP_PRECISION_MIXED 1
 #define CP_PERSISTENT_MAX_DOFS 49152
 typedef struct cp_solve_info_t {
-    int32_t iterations; /* Krylov iterations to convergence (or the cap) */
+    int32_t iterations; /* Krylov iterations to convergence (or the cap); mixed precision: all
+                           inner FP32 iterations of every refinement pass */
     int32_t converged;  /* 1 if the tolerance was met */
     int32_t breakdown;  /* 1 if the method broke down (zero rho or denominator) */
-    int32_t reserved;
+    int32_t refinements; /* mixed precision: refinement passes run (0 in FP64) */
     double rhs_norm;      /* ||b|| of the condensed system */
     double residual_norm; /* the tested residual norm at exit */
 } cp_solve_info_t;
@@ -318,6 +353,51 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
  * cp_averages / cp_reorient / cp_commit as after cp_update.
  */
 int cp_update_from_displacement(cp_handle* h, double F_e, double F_r);
+
+/*
+ * Launch-shape autotuner of the sorted update (no counterpart in the
+ * reference).  Shapes (threads per block / registers per thread):
+ *   0: 256 / 255   1: 256 / 128   2: 64 / 255   3: 64 / 128
+ * The untuned rule takes 2 (FCC class) or 3 (BCC/HCP classes) for launches
+ * of at most 9,472 qps and 0 or 1 above.  cp_autotune times every shape on
+ * the live workload, group by group: path CP_TUNE_UPDATE runs the flag-1
+ * update with d_in = F (9*n_qp, device); path CP_TUNE_ASSEMBLE runs the fused
+ * assembly's update with d_in = U_local (24*n_cells, device).  Each shape
+ * runs 1 + reps times (the first untimed); the update reads the _conv
+ * history and writes _iter, so the repeats see the same input and leave the
+ * history as one call would.  The chosen shape (cp_tune_select on the
+ * timings, min_gain as there) is stored in the handle for that path and
+ * used by later calls while cp_options_t.update_variant is 0.  results (may
+ * be NULL) receives one row per lattice group; returns the number of groups
+ * or a negative CP_E* code.  Synchronous.
+ */
+#define CP_UPDATE_VARIANTS 4
+#define CP_TUNE_UPDATE 0
+#define CP_TUNE_ASSEMBLE 1
+typedef struct cp_tune_result_t {
+    int32_t lattice;         /* lattice id of the group */
+    int32_t chosen;          /* shape chosen, 0..CP_UPDATE_VARIANTS-1 */
+    int32_t default_variant; /* the untuned rule's shape for the group */
+    int32_t reserved;
+    int64_t n_qp;            /* qps of the group */
+    double median_ms[CP_UPDATE_VARIANTS]; /* median time of one launch per shape */
+} cp_tune_result_t;
+int cp_autotune(cp_handle* h, const double* d_in, int32_t path, int32_t reps, double min_gain,
+                cp_tune_result_t* results, int32_t max_results);
+
+/*
+ * The autotuner's selection rule, host only: ms[v * reps + r] is repeat r of
+ * shape v (non-finite or negative entries are failed launches and count as
+ * missing).  Picks the shape with the smallest median (ties: the lower
+ * index), but keeps default_variant unless the winner's median is below
+ * (1 - min_gain) times the default's.  Returns -1 if no shape has a timing.
+ */
+int32_t cp_tune_select(int32_t n_variants, int32_t reps, const double* ms, int32_t default_variant,
+                       double min_gain);
+
+/* CUDA graphs captured (instantiated or updated) and launched by the handle
+ * since its creation (cp_options_t.use_graphs). */
+int cp_graph_stats(cp_handle* h, int64_t* captures, int64_t* launches);
 
 /* Wait for all work queued on the handle's stream. */
 int cp_synchronize(cp_handle* h);

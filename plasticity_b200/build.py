@@ -2,29 +2,51 @@
 
 The product is a plain C-ABI shared library (include/cp_gpu.h); Python loads
 it with ctypes.  Built with nvcc directly, so the .so lives in the source
-tree and travels with it.
+tree and travels with it.  The large per-qp kernels are separate translation
+units (one per lattice class, F source and launch shape of the sorted update;
+one per lattice class of the plain kernels) compiled in parallel and linked
+into the one library.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
+OBJ_DIR = os.path.join(OUT_DIR, "obj")
 LIB = os.path.join(OUT_DIR, "libcp_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "cp_api.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
-    os.path.join(ROOT, "include", "cp_gpu.h")]
 
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
     "-I" + os.path.join(ROOT, "include"),
 ]
+
+U2_VARIANTS = 4  # kU2Shapes in csrc/cp_launch.h
+
+
+def units():
+    """(object name, source, extra defines) of every translation unit."""
+    out = [("cp_api", "cp_api.cu", []), ("cp_tc", "cp_tc.cu", [])]
+    for pmax in (16, 32, 48):
+        for fsrc in ("FromArray", "FromMesh"):
+            for v in range(U2_VARIANTS):
+                out.append((f"u2_{pmax}_{fsrc}_{v}", "cp_update_tu.cu",
+                            [f"-DCP_TU_PMAX={pmax}", f"-DCP_TU_FSRC={fsrc}", f"-DCP_TU_VARIANT={v}"]))
+    for nt, pmax in ((16, 16), (32, 32), (64, 48)):
+        out.append((f"plain_{nt}", "cp_plain_tu.cu", [f"-DCP_TU_NT={nt}", f"-DCP_TU_PMAX={pmax}"]))
+    return [u for u in out if os.path.exists(os.path.join(CSRC, u[1]))]
+
+
+def deps():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "cp_gpu.h")]
 
 
 def nvcc():
@@ -34,26 +56,51 @@ def nvcc():
     return "nvcc"
 
 
+def _newest_dep() -> float:
+    return max(os.path.getmtime(d) for d in deps() if os.path.exists(d))
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(d) <= t for d in DEPS if os.path.exists(d))
+    return _newest_dep() <= os.path.getmtime(LIB)
 
 
-def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+def _obj(name):
+    return os.path.join(OBJ_DIR, name + ".o")
+
+
+def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | None = None) -> str:
     if not force and up_to_date():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + SOURCES + ["-o", LIB]
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    newest = _newest_dep()
+    todo = [u for u in units()
+            if force or extra or not os.path.exists(_obj(u[0])) or os.path.getmtime(_obj(u[0])) < newest]
+
+    def compile_one(u):
+        name, src, defs = u
+        cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + defs + ["-c", os.path.join(CSRC, src), "-o", _obj(name)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return name, cmd, r
+
+    failed = []
+    with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        for name, cmd, r in ex.map(compile_one, todo):
+            if verbose:
+                print(" ".join(cmd))
+                if r.stdout or r.stderr:
+                    print(r.stdout + r.stderr)
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                failed.append(name)
+    if failed:
+        raise RuntimeError("nvcc failed: " + ", ".join(failed))
+    link = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC"] + [_obj(u[0]) for u in units()] + ["-o", LIB]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed")
-    if verbose and (r.stdout or r.stderr):
-        print(r.stdout + r.stderr)
+        raise RuntimeError("nvcc link failed")
     return LIB
 
 

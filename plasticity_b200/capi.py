@@ -78,7 +78,7 @@ class CpOptions(C.Structure):
         ("max_solver_iterations", C.c_int32),
         ("enable_multiphase", C.c_int32),
         ("device", C.c_int32),
-        ("block_size", C.c_int32),
+        ("update_variant", C.c_int32),
         ("use_graphs", C.c_int32),
         ("plain_kernel", C.c_int32),
     ]
@@ -95,6 +95,8 @@ class CpSolver(C.Structure):
         ("check_every", C.c_int32),
         ("precond", C.c_int32),
         ("kernel_mode", C.c_int32),
+        ("precision", C.c_int32),
+        ("max_refinements", C.c_int32),
     ]
 
 
@@ -103,9 +105,29 @@ class CpSolveInfo(C.Structure):
         ("iterations", C.c_int32),
         ("converged", C.c_int32),
         ("breakdown", C.c_int32),
-        ("reserved", C.c_int32),
+        ("refinements", C.c_int32),
         ("rhs_norm", C.c_double),
         ("residual_norm", C.c_double),
+    ]
+
+
+CP_UPDATE_VARIANTS = 4
+CP_TUNE_UPDATE = 0
+CP_TUNE_ASSEMBLE = 1
+# launch shapes of the sorted update: (threads per block, registers per thread)
+UPDATE_SHAPES = [(256, 255), (256, 128), (64, 255), (64, 128)]
+
+
+class CpTuneResult(C.Structure):
+    """cp_tune_result_t: one lattice group's autotuning outcome."""
+
+    _fields_ = [
+        ("lattice", C.c_int32),
+        ("chosen", C.c_int32),
+        ("default_variant", C.c_int32),
+        ("reserved", C.c_int32),
+        ("n_qp", C.c_int64),
+        ("median_ms", C.c_double * CP_UPDATE_VARIANTS),
     ]
 
 
@@ -113,6 +135,8 @@ CP_SOLVER_BICG = 0
 CP_SOLVER_BICGSTAB = 1
 CP_PRECOND_JACOBI = 0
 CP_PRECOND_NODE_BLOCK = 1
+CP_PRECISION_FP64 = 0
+CP_PRECISION_MIXED = 1
 
 
 def default_solver(**kw) -> CpSolver:
@@ -133,8 +157,8 @@ def default_options(**kw) -> CpOptions:
     o.max_solver_iterations = 1
     o.enable_multiphase = 0
     o.device = 0
-    o.block_size = 0
-    o.use_graphs = 0
+    o.update_variant = 0
+    o.use_graphs = 1
     o.plain_kernel = 0
     for k, v in kw.items():
         setattr(o, k, v)
@@ -203,6 +227,9 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_assemble": (C.c_int, [H, D, C.c_double, C.c_double, D, D, I32]),
         "cp_assemble_device": (C.c_int, [H, C.c_void_p, C.c_double, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cp_assemble_mixed": (C.c_int, [H, D, C.c_double, C.c_double, C.POINTER(C.c_float), D, I32]),
+        "cp_assemble_mixed_device": (C.c_int, [H, C.c_void_p, C.c_double, C.c_double,
+                                               C.c_void_p, C.c_void_p, C.c_void_p]),
         "cp_averages": (C.c_int, [H, D]),
         "cp_averages_noalloc": (C.c_int, [H, D]),
         "cp_reorient": (C.c_int, [H]),
@@ -215,6 +242,10 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_measure_fp64_peak": (C.c_int, [C.c_int32, D]),
         "cp_set_timing": (C.c_int, [H, C.c_int32]),
         "cp_get_timing": (C.c_int, [H, C.c_int32, I32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), D]),
+        "cp_autotune": (C.c_int, [H, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(CpTuneResult),
+                                  C.c_int32]),
+        "cp_tune_select": (C.c_int32, [C.c_int32, C.c_int32, D, C.c_int32, C.c_double]),
+        "cp_graph_stats": (C.c_int, [H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -315,6 +346,16 @@ class CpHandle:
                     "cp_assemble")
         return Ke, Re, st
 
+    def assemble_mixed(self, U_local, F_e: float = 0.0, F_r: float = 0.0):
+        """cp_assemble_mixed: FP32 Ke from the split-BF16 tensor-core contraction, FP64 Re."""
+        U = as_f64(U_local, (self.n_cells, 24))
+        Ke = np.empty((self.n_cells, 24, 24), dtype=np.float32)
+        Re = np.empty((self.n_cells, 24))
+        st = np.empty(self.n_qp, dtype=np.int32)
+        self._check(self.lib.cp_assemble_mixed(self.h, dptr(U), F_e, F_r, Ke.ctypes.data_as(C.POINTER(C.c_float)),
+                                               dptr(Re), iptr(st)), "cp_assemble_mixed")
+        return Ke, Re, st
+
     def assemble_device(self, U_ptr, F_e, F_r, Ke_ptr, Re_ptr, status_ptr=None):
         self._check(self.lib.cp_assemble_device(self.h, C.c_void_p(U_ptr), F_e, F_r, C.c_void_p(Ke_ptr),
                                                 C.c_void_p(Re_ptr),
@@ -352,7 +393,7 @@ class CpHandle:
                                                  C.byref(solver) if solver is not None else None,
                                                  C.byref(info)), "cp_newton_iteration")
         return {"iterations": info.iterations, "converged": bool(info.converged), "breakdown": bool(info.breakdown),
-                "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
+                "refinements": info.refinements, "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
 
     def update_from_displacement(self, F_e: float = 0.0, F_r: float = 0.0):
         self._check(self.lib.cp_update_from_displacement(self.h, F_e, F_r), "cp_update_from_displacement")
@@ -385,6 +426,22 @@ class CpHandle:
 
     def set_timing(self, enable: bool):
         self._check(self.lib.cp_set_timing(self.h, 1 if enable else 0), "cp_set_timing")
+
+    def autotune(self, in_ptr: int, path: int = CP_TUNE_UPDATE, reps: int = 3, min_gain: float = 0.02):
+        """cp_autotune on device input (F for CP_TUNE_UPDATE, U_local for CP_TUNE_ASSEMBLE): one dict per
+        lattice group with the shape chosen, the untuned default and the median ms of every shape."""
+        res = (CpTuneResult * CP_MAX_LATTICES)()
+        ng = self.lib.cp_autotune(self.h, C.c_void_p(in_ptr), path, reps, min_gain, res, CP_MAX_LATTICES)
+        if ng < 0:
+            self._check(ng, "cp_autotune")
+        return [{"lattice": res[g].lattice, "n_qp": res[g].n_qp, "chosen": res[g].chosen,
+                 "default": res[g].default_variant, "median_ms": list(res[g].median_ms)} for g in range(ng)]
+
+    def graph_stats(self):
+        """(graphs captured, graph launches) since the handle was created."""
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self.lib.cp_graph_stats(self.h, C.byref(a), C.byref(b)), "cp_graph_stats")
+        return int(a.value), int(b.value)
 
     def get_timing(self):
         """[(lattice, qp count, launches, total ms)] per internal group."""

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <type_traits>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -11,6 +13,7 @@
 
 #include "../../include/cp_gpu.h"
 #include "cp_kernels.cuh"
+#include "cp_launch.h"
 #include "cp_solve.cuh"
 
 using namespace cp;
@@ -229,6 +232,17 @@ __global__ void scatter_field_kernel(double* __restrict__ dst, int* __restrict__
     }
 }
 
+// F of every qp from the cell's nodal displacements (getElementalValues.cc:129-138),
+// the same expression the sorted update evaluates inline (FromMesh), for the
+// plain kernel's post-pass from the device displacement
+__global__ void mesh_F_kernel(FromMesh fm, int64_t n_qp, double* __restrict__ F) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_qp) return;
+    const M3 f = fm(k);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) F[9 * k + c] = f.a[c];
+}
+
 // FP64 FMA throughput probe: 8 independent dependent-FMA chains per thread.
 __global__ void fp64_fma_probe_kernel(int iters, double seed, double* out) {
     double a[8];
@@ -269,6 +283,8 @@ struct Group {
     unsigned char* d_key = nullptr;  // sort key per internal qp
     int* d_perm = nullptr;           // internal qps in sorted order
     int* d_hist = nullptr;           // SORT_BUCKETS counts, then SORT_BUCKETS offsets
+    int tuned[2] = {-1, -1};         // launch shape chosen by cp_autotune (F from an array / from the
+                                     // mesh); -1: the default rule of u2_default_variant
     GroupDev dev{};
     std::vector<int64_t> qp_host;    // host copy of d_qp (increasing caller indices)
 };
@@ -308,6 +324,8 @@ struct cp_handle {
     double *d_gradN = nullptr, *d_JxW = nullptr;
     double *d_U = nullptr, *d_Ke = nullptr, *d_Re = nullptr;
     double* d_stage = nullptr;  // JxW*P and JxW*dP/dF per qp between update and contraction
+    int num_sms = 0;
+    int* d_tc_err = nullptr;    // raised by the tensor-core contraction if one of its waits expired
     // global system of the Newton step (cp_bind_dofs)
     struct System {
         int64_t n_dofs = 0, nnz = 0, n_con = 0;
@@ -350,6 +368,31 @@ struct cp_handle {
     std::vector<Pending> pending;
     std::vector<double> group_ms;
     std::vector<int64_t> group_launches;
+    // captured calls (cp_options_t.use_graphs): a few graphs keyed by the
+    // call's kind, pointers, scalars and launch shapes, least recently used
+    // replaced first
+    struct GraphKey {
+        int kind = -1;
+        const void* p[8] = {};
+        int flag = 0;
+        uint64_t fe = 0, fr = 0;
+        int64_t epoch = 0;  // tune_epoch at capture
+        bool operator==(const GraphKey& o) const {
+            if (kind != o.kind || flag != o.flag || fe != o.fe || fr != o.fr || epoch != o.epoch) return false;
+            for (int i = 0; i < 8; ++i)
+                if (p[i] != o.p[i]) return false;
+            return true;
+        }
+    };
+    struct GraphEntry {
+        GraphKey key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t last_use = 0;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t graph_clock = 0;
+    int64_t graph_captures = 0, graph_launches = 0;
+    int64_t tune_epoch = 0;  // bumped whenever a group's launch shape changes
     std::string err;
 };
 
@@ -382,7 +425,14 @@ void free_group(Group& g) {
     g = Group{};
 }
 
+void free_graphs(cp_handle* h) {
+    for (auto& e : h->graphs)
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+    h->graphs.clear();
+}
+
 void free_qps(cp_handle* h) {
+    free_graphs(h);
     for (auto& g : h->groups) free_group(g);
     h->groups.clear();
     cudaFree(h->d_F);
@@ -405,6 +455,7 @@ void free_qps(cp_handle* h) {
 void free_system(cp_handle* h);
 
 void free_mesh(cp_handle* h) {
+    free_graphs(h);
     free_system(h);
     cudaFree(h->d_gradN);
     cudaFree(h->d_JxW);
@@ -492,24 +543,37 @@ void carve(Group& g) {
 
 unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
-template <int NT, int PMAX>
-void launch_update(cp_handle* h, const Group& g, const double* F, int flag, double F_e, double F_r, double* P,
-                   double* T, double* dPdF, int32_t* st, double* kF, double* kT) {
-    update_kernel<NT, PMAX><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(
-        h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P, T, dPdF, st, h->d_stats, kF, kT, g.lattice);
+void launch_update_plain_group(cp_handle* h, const Group& g, const double* F, int flag, double F_e, double F_r,
+                               double* P, double* T, double* dPdF, int32_t* st, double* kF, double* kT) {
+    switch (g.nt_class) {
+        case 16:
+            launch_update_plain<16, 16>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P, T, dPdF,
+                                        st, h->d_stats, kF, kT, g.lattice);
+            break;
+        case 32:
+            launch_update_plain<32, 32>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P, T, dPdF,
+                                        st, h->d_stats, kF, kT, g.lattice);
+            break;
+        default:
+            launch_update_plain<64, 48>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P, T, dPdF,
+                                        st, h->d_stats, kF, kT, g.lattice);
+            break;
+    }
 }
 
-template <int NT, int PMAX>
-cudaError_t launch_assemble(cp_handle* h, const Group& g, const double* U, double F_e, double F_r, double* Ke,
-                            double* Re, int32_t* st) {
-    const size_t smem = (size_t)QP_BLOCK * 90 * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(assemble_kernel<NT, PMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    assemble_kernel<NT, PMAX><<<blocks_for(g.count, QP_BLOCK), QP_BLOCK, smem, h->stream>>>(
-        h->d_lat[g.lattice], h->dopts, g.dev, U, h->d_gradN, h->d_JxW, h->uniform, F_e, F_r, Ke, Re, st,
-        h->d_stats, g.lattice);
-    return cudaGetLastError();
+cudaError_t launch_assemble_plain_group(cp_handle* h, const Group& g, const double* U, double F_e, double F_r,
+                                        double* Ke, double* Re, int32_t* st) {
+    switch (g.nt_class) {
+        case 16:
+            return launch_assemble_plain<16, 16>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, U, h->d_gradN,
+                                                 h->d_JxW, h->uniform, F_e, F_r, Ke, Re, st, h->d_stats, g.lattice);
+        case 32:
+            return launch_assemble_plain<32, 32>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, U, h->d_gradN,
+                                                 h->d_JxW, h->uniform, F_e, F_r, Ke, Re, st, h->d_stats, g.lattice);
+        default:
+            return launch_assemble_plain<64, 48>(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, U, h->d_gradN,
+                                                 h->d_JxW, h->uniform, F_e, F_r, Ke, Re, st, h->d_stats, g.lattice);
+    }
 }
 
 void timing_begin(cp_handle* h, int gi, cudaEvent_t* a) {
@@ -538,18 +602,38 @@ void sort_group(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m) {
                                                                     g.d_perm + i0);
 }
 
+template <class FSrc>
+constexpr int fsrc_path() {
+    return std::is_same<FSrc, FromMesh>::value ? 1 : 0;
+}
+
 template <int PMAX, class FSrc>
-void launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m, int flag, double F_e, double F_r,
-                    double* P, double* T, double* dPdF, double* stage, int32_t* st, double* kF, double* kT) {
-    if (m <= UPDATE2_SPREAD_QPS)
-        update2_kernel<PMAX, FSrc, UPDATE2_SPREAD_BLOCK, update2_spread_min_blocks(PMAX)>
-            <<<blocks_for(m, UPDATE2_SPREAD_BLOCK), UPDATE2_SPREAD_BLOCK, 0, h->stream>>>(
-                h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
-                h->d_stats, kF, kT, g.lattice);
-    else
-        update2_kernel<PMAX, FSrc><<<blocks_for(m, update2_block(PMAX)), update2_block(PMAX), 0, h->stream>>>(
-            h->d_lat[g.lattice], h->dopts, g.dev, fs, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
-            h->d_stats, kF, kT, g.lattice);
+cudaError_t launch_update2_shape(cudaStream_t s, const U2Args& a, const FSrc& fs, int v) {
+    switch (v) {
+        case 0: return launch_update2_v<PMAX, FSrc, 0>(s, a, fs);
+        case 1: return launch_update2_v<PMAX, FSrc, 1>(s, a, fs);
+        case 2: return launch_update2_v<PMAX, FSrc, 2>(s, a, fs);
+        default: return launch_update2_v<PMAX, FSrc, 3>(s, a, fs);
+    }
+}
+
+// the sorted update of internal qps [i0, i0 + m) of group g (sort done) in
+// launch shape v (-1: the group's tuned shape, else the default rule)
+template <class FSrc>
+cudaError_t launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m, int flag, double F_e,
+                           double F_r, double* P, double* T, double* dPdF, double* stage, int32_t* st, double* kF,
+                           double* kT, int v = -1) {
+    const int pmax = g.nt_class == 16 ? 16 : (g.nt_class == 32 ? 32 : 48);
+    if (v < 0 && h->opts.update_variant > 0) v = h->opts.update_variant - 1;
+    if (v < 0) v = g.tuned[fsrc_path<FSrc>()];
+    if (v < 0) v = u2_default_variant(pmax, m);
+    const U2Args a{h->d_lat[g.lattice], h->dopts, g.dev, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
+                   h->d_stats, kF, kT, g.lattice};
+    switch (pmax) {
+        case 16: return launch_update2_shape<16>(h->stream, a, fs, v);
+        case 32: return launch_update2_shape<32>(h->stream, a, fs, v);
+        default: return launch_update2_shape<48>(h->stream, a, fs, v);
+    }
 }
 
 // calculatePlasticity over internal qps [i0, i0 + m) of group gi (sort + update)
@@ -563,12 +647,78 @@ void sorted_update_group(cp_handle* h, size_t gi, FSrc fs, int flag, double F_e,
     sort_group(h, g, fs, i0, m);
     cudaEvent_t ev{};
     timing_begin(h, (int)gi, &ev);
-    switch (g.nt_class) {
-        case 16: launch_update2<16>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
-        case 32: launch_update2<32>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
-        default: launch_update2<48>(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT); break;
-    }
+    launch_update2(h, g, fs, i0, m, flag, F_e, F_r, P, T, dPdF, stage, st, kF, kT);
     timing_end(h, (int)gi, ev);
+}
+
+uint64_t bits_of(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, sizeof u);
+    return u;
+}
+
+// Run enqueue() (the stream work of one call) through a CUDA graph captured
+// for this key: captured on first use (or when the key changes: the cached
+// graph is updated in place when its topology allows, else re-instantiated)
+// and launched with one cudaGraphLaunch.  Without use_graphs, with launch
+// timing on, or when the stream is already being captured by the caller, the
+// work is enqueued directly.
+template <class Enqueue>
+int run_graph(cp_handle* h, const cp_handle::GraphKey& key, Enqueue enqueue) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(h, cudaStreamIsCapturing(h->stream, &cs));
+    if (!h->opts.use_graphs || h->timing || cs != cudaStreamCaptureStatusNone) return enqueue();
+    cp_handle::GraphEntry* hit = nullptr;
+    for (auto& e : h->graphs)
+        if (e.exec && e.key == key) hit = &e;
+    if (!hit) {
+        CK(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (rc != CP_OK || e != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != CP_OK ? rc : cuda_fail(h, e == cudaSuccess ? cudaErrorUnknown : e, "graph capture");
+        }
+        // a slot: an unused one, else the least recently used (updated in
+        // place if the topology matches, else re-instantiated)
+        constexpr size_t MAX_GRAPHS = 6;
+        if (h->graphs.size() < MAX_GRAPHS) {
+            h->graphs.emplace_back();
+            hit = &h->graphs.back();
+        } else {
+            hit = &h->graphs[0];
+            for (auto& x : h->graphs)
+                if (x.last_use < hit->last_use) hit = &x;
+        }
+        bool ok = false;
+        if (hit->exec) {
+            cudaGraphExecUpdateResultInfo info;
+            ok = cudaGraphExecUpdate(hit->exec, g, &info) == cudaSuccess;
+            if (!ok) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(hit->exec);
+                hit->exec = nullptr;
+            }
+        }
+        if (!ok) {
+            const cudaError_t ei = cudaGraphInstantiate(&hit->exec, g, 0);
+            if (ei != cudaSuccess) {
+                hit->exec = nullptr;
+                hit->key = cp_handle::GraphKey{};
+                cudaGraphDestroy(g);
+                return cuda_fail(h, ei, "cudaGraphInstantiate");
+            }
+        }
+        cudaGraphDestroy(g);
+        hit->key = key;
+        ++h->graph_captures;
+    }
+    hit->last_use = ++h->graph_clock;
+    CK(h, cudaGraphLaunch(hit->exec, h->stream));
+    ++h->graph_launches;
+    return CP_OK;
 }
 
 int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double F_r, double* P, double* T,
@@ -576,9 +726,24 @@ int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double 
     if (!h->opts.plain_kernel) {
         double* kF = flag == 0 ? h->d_keepF : nullptr;
         double* kT = flag == 0 ? h->d_keepT : nullptr;
-        for (size_t gi = 0; gi < h->groups.size(); ++gi)
-            sorted_update_group(h, gi, FromArray{F}, flag, F_e, F_r, P, T, dPdF, nullptr, st, kF, kT);
-        CK(h, cudaGetLastError());
+        cp_handle::GraphKey key;
+        key.kind = 0;
+        key.p[0] = F;
+        key.p[1] = P;
+        key.p[2] = T;
+        key.p[3] = dPdF;
+        key.p[4] = st;
+        key.flag = flag;
+        key.fe = bits_of(F_e);
+        key.fr = bits_of(F_r);
+        key.epoch = h->tune_epoch;
+        const int rc = run_graph(h, key, [&]() -> int {
+            for (size_t gi = 0; gi < h->groups.size(); ++gi)
+                sorted_update_group(h, gi, FromArray{F}, flag, F_e, F_r, P, T, dPdF, nullptr, st, kF, kT);
+            CK(h, cudaGetLastError());
+            return CP_OK;
+        });
+        if (rc != CP_OK) return rc;
         if (flag == 0) h->have_post = true;
         return CP_OK;
     }
@@ -588,11 +753,7 @@ int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double 
         const auto& g = h->groups[gi];
         cudaEvent_t ev{};
         timing_begin(h, (int)gi, &ev);
-        switch (g.nt_class) {
-            case 16: launch_update<16, 16>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
-            case 32: launch_update<32, 32>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
-            default: launch_update<64, 48>(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT); break;
-        }
+        launch_update_plain_group(h, g, F, flag, F_e, F_r, P, T, dPdF, st, kF, kT);
         timing_end(h, (int)gi, ev);
     }
     CK(h, cudaGetLastError());
@@ -618,7 +779,7 @@ int cp_options_default(cp_options_t* o) {
     o->max_solver_iterations = 1;
     o->enable_multiphase = 0;
     o->device = 0;
-    o->block_size = 0;
+    o->update_variant = 0;
     o->use_graphs = 1;
     return CP_OK;
 }
@@ -677,6 +838,12 @@ int cp_create(const cp_material_t* lattices, int32_t n_lattices, const cp_option
         cp_destroy(h);
         return CP_E_CUDA;
     }
+    if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess ||
+        prepare_ke_tc() != cudaSuccess || cudaMalloc(&h->d_tc_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(h->d_tc_err, 0, sizeof(int)) != cudaSuccess) {
+        cp_destroy(h);
+        return CP_E_CUDA;
+    }
     h->dopts.tol = h->opts.stress_tolerance;
     h->dopts.max_search = h->opts.max_slip_search_iterations;
     h->dopts.max_solver = h->opts.max_solver_iterations;
@@ -728,6 +895,7 @@ void cp_destroy(cp_handle* h) {
     free_mesh(h);
     cudaFree(h->d_avg_partial);
     cudaFree(h->d_avg_out);
+    cudaFree(h->d_tc_err);
     for (auto* d : h->d_lat) cudaFree(d);
     for (auto& p : h->pending) {
         cudaEventDestroy(p.a);
@@ -933,24 +1101,31 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
         if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
             return fail(h, CP_E_NOMEM, "cp_assemble: staging allocation failed");
         const FromMesh fm{d_U, h->d_gradN, h->d_JxW, h->uniform};
-        for (size_t gi = 0; gi < h->groups.size(); ++gi)
-            sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status, nullptr,
-                                nullptr);
-        contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
-            h->d_stage, h->d_gradN, h->uniform, 0, h->n_cells, d_Ke, d_Re);
-        CK(h, cudaGetLastError());
-        return CP_OK;
+        cp_handle::GraphKey key;
+        key.kind = 1;
+        key.p[0] = d_U;
+        key.p[1] = d_Ke;
+        key.p[2] = d_Re;
+        key.p[3] = d_status;
+        key.flag = 1;
+        key.fe = bits_of(F_e);
+        key.fr = bits_of(F_r);
+        key.epoch = h->tune_epoch;
+        return run_graph(h, key, [&]() -> int {
+            for (size_t gi = 0; gi < h->groups.size(); ++gi)
+                sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status,
+                                    nullptr, nullptr);
+            contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
+                h->d_stage, h->d_gradN, h->uniform, 0, h->n_cells, d_Ke, d_Re);
+            CK(h, cudaGetLastError());
+            return CP_OK;
+        });
     }
     for (size_t gi = 0; gi < h->groups.size(); ++gi) {
         const auto& g = h->groups[gi];
         cudaEvent_t ev{};
         timing_begin(h, (int)gi, &ev);
-        cudaError_t e;
-        switch (g.nt_class) {
-            case 16: e = launch_assemble<16, 16>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
-            case 32: e = launch_assemble<32, 32>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
-            default: e = launch_assemble<64, 48>(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status); break;
-        }
+        const cudaError_t e = launch_assemble_plain_group(h, g, d_U, F_e, F_r, d_Ke, d_Re, d_status);
         timing_end(h, (int)gi, ev);
         if (e != cudaSuccess) return cuda_fail(h, e, "assemble_kernel");
     }
@@ -1019,6 +1194,73 @@ int cp_assemble(cp_handle* h, const double* h_U, double F_e, double F_r, double*
     CK(h, cudaStreamSynchronize(h->s_out));
     CK(h, cudaStreamSynchronize(h->stream));
     return CP_OK;
+}
+
+// reads and clears the tensor-core contraction's error flag (synchronises)
+static int check_tc_error(cp_handle* h) {
+    int e = 0;
+    CK(h, cudaMemcpyAsync(&e, h->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (e) {
+        CK(h, cudaMemsetAsync(h->d_tc_err, 0, sizeof(int), h->stream));
+        return fail(h, CP_E_CUDA, "tensor-core contraction: a wait expired (results incomplete)");
+    }
+    return CP_OK;
+}
+
+int cp_assemble_mixed_device(cp_handle* h, const double* d_U, double F_e, double F_r, float* d_Ke, double* d_Re,
+                             int32_t* d_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble_mixed: no mesh bound");
+    if (!d_U || !d_Ke || !d_Re) return fail(h, CP_E_ARG, "cp_assemble_mixed: bad arguments");
+    if (!h->uniform) return fail(h, CP_E_UNSUPPORTED, "cp_assemble_mixed: needs a uniform mesh (shared gradients)");
+    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_assemble_mixed: needs the sorted update");
+    if (int rc = check_device(h)) return rc;
+    if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_assemble_mixed: staging allocation failed");
+    const FromMesh fm{d_U, h->d_gradN, h->d_JxW, h->uniform};
+    cp_handle::GraphKey key;
+    key.kind = 3;
+    key.p[0] = d_U;
+    key.p[1] = d_Ke;
+    key.p[2] = d_Re;
+    key.p[3] = d_status;
+    key.flag = 1;
+    key.fe = bits_of(F_e);
+    key.fr = bits_of(F_r);
+    key.epoch = h->tune_epoch;
+    return run_graph(h, key, [&]() -> int {
+        for (size_t gi = 0; gi < h->groups.size(); ++gi)
+            sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status, nullptr,
+                                nullptr);
+        CK(h, cudaGetLastError());
+        CK(h, launch_ke_tc(h->stream, h->d_stage, h->d_gradN, 0, h->n_cells, d_Ke, d_Re, h->d_tc_err, h->num_sms));
+        return CP_OK;
+    });
+}
+
+int cp_assemble_mixed(cp_handle* h, const double* h_U, double F_e, double F_r, float* h_Ke, double* h_Re,
+                      int32_t* h_status) {
+    if (!h) return CP_E_ARG;
+    if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble_mixed: no mesh bound");
+    if (!h_U || !h_Ke || !h_Re) return fail(h, CP_E_ARG, "cp_assemble_mixed: bad arguments");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    const int64_t nc = h->n_cells;
+    if (!h->d_U) {
+        if (cudaMalloc(&h->d_U, sizeof(double) * 24 * nc) != cudaSuccess ||
+            cudaMalloc(&h->d_Ke, sizeof(double) * 576 * nc) != cudaSuccess ||
+            cudaMalloc(&h->d_Re, sizeof(double) * 24 * nc) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "cp_assemble_mixed: allocation failed");
+    }
+    float* dK = reinterpret_cast<float*>(h->d_Ke);  // FP32 Ke in the first half of the FP64 buffer
+    CK(h, cudaMemcpyAsync(h->d_U, h_U, sizeof(double) * 24 * nc, cudaMemcpyHostToDevice, h->stream));
+    if (int rc = cp_assemble_mixed_device(h, h->d_U, F_e, F_r, dK, h->d_Re, h->d_status)) return rc;
+    CK(h, cudaMemcpyAsync(h_Ke, dK, sizeof(float) * 576 * nc, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(h_Re, h->d_Re, sizeof(double) * 24 * nc, cudaMemcpyDeviceToHost, h->stream));
+    if (h_status)
+        CK(h, cudaMemcpyAsync(h_status, h->d_status, sizeof(int32_t) * h->n_qp, cudaMemcpyDeviceToHost, h->stream));
+    return check_tc_error(h);
 }
 
 int cp_averages(cp_handle* h, double out[22]) {
@@ -1296,7 +1538,7 @@ int cp_synchronize(cp_handle* h) {
     if (!h) return CP_E_ARG;
     if (int rc = check_device(h)) return rc;
     CK(h, cudaStreamSynchronize(h->stream));
-    return CP_OK;
+    return check_tc_error(h);
 }
 
 // ---- the Newton step's global system ------------------------------------
@@ -1774,19 +2016,146 @@ int cp_update_from_displacement(cp_handle* h, double F_e, double F_r) {
     if (!h) return CP_E_ARG;
     auto& s = h->sys;
     if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_update_from_displacement: no dofs bound");
-    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_update_from_displacement: needs the sorted update");
     if (int rc = check_device(h)) return rc;
     if (int rc = ensure_staging(h, false)) return rc;
     const int64_t nc = h->n_cells;
-    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
-        s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
     const FromMesh fm{s.d_Ul, h->d_gradN, h->d_JxW, h->uniform};
-    for (size_t gi = 0; gi < h->groups.size(); ++gi)
-        sorted_update_group(h, gi, fm, 0, F_e, F_r, nullptr, nullptr, nullptr, nullptr, h->d_status, h->d_keepF,
-                            h->d_keepT);
-    CK(h, cudaGetLastError());
+    if (h->opts.plain_kernel) {  // F of every qp first, then the plain update on it
+        gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+            s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
+        mesh_F_kernel<<<blocks_for(h->n_qp, 256), 256, 0, h->stream>>>(fm, h->n_qp, h->d_F);
+        CK(h, cudaGetLastError());
+        return dispatch_update(h, h->d_F, 0, F_e, F_r, nullptr, nullptr, nullptr, h->d_status);
+    }
+    cp_handle::GraphKey key;
+    key.kind = 2;
+    key.fe = bits_of(F_e);
+    key.fr = bits_of(F_r);
+    key.epoch = h->tune_epoch;
+    const int rc = run_graph(h, key, [&]() -> int {
+        gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+            s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
+        for (size_t gi = 0; gi < h->groups.size(); ++gi)
+            sorted_update_group(h, gi, fm, 0, F_e, F_r, nullptr, nullptr, nullptr, nullptr, h->d_status, h->d_keepF,
+                                h->d_keepT);
+        CK(h, cudaGetLastError());
+        return CP_OK;
+    });
+    if (rc != CP_OK) return rc;
     h->have_post = true;
     return CP_OK;
 }
 
+int32_t cp_tune_select(int32_t n_variants, int32_t reps, const double* ms, int32_t default_variant,
+                       double min_gain) {
+    if (n_variants < 1 || reps < 1 || !ms) return -1;
+    std::vector<double> med(n_variants, 0.0);
+    std::vector<bool> valid(n_variants, false);
+    for (int v = 0; v < n_variants; ++v) {
+        std::vector<double> x;
+        for (int r = 0; r < reps; ++r) {
+            const double t = ms[(int64_t)v * reps + r];
+            if (std::isfinite(t) && t >= 0.0) x.push_back(t);
+        }
+        if (x.empty()) continue;
+        std::sort(x.begin(), x.end());
+        const size_t c = x.size();
+        med[v] = c % 2 ? x[c / 2] : 0.5 * (x[c / 2 - 1] + x[c / 2]);
+        valid[v] = true;
+    }
+    int best = -1;
+    for (int v = 0; v < n_variants; ++v)
+        if (valid[v] && (best < 0 || med[v] < med[best])) best = v;
+    if (best < 0) return -1;
+    if (default_variant >= 0 && default_variant < n_variants && valid[default_variant] && best != default_variant &&
+        !(med[best] < (1.0 - min_gain) * med[default_variant]))
+        return default_variant;
+    return best;
+}
+
+int cp_autotune(cp_handle* h, const double* d_in, int32_t path, int32_t reps, double min_gain,
+                cp_tune_result_t* results, int32_t max_results) {
+    if (!h) return CP_E_ARG;
+    if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_autotune: no qps bound");
+    if (!d_in || (path != CP_TUNE_UPDATE && path != CP_TUNE_ASSEMBLE) || reps < 1 || reps > 64 ||
+        !(min_gain >= 0.0 && min_gain < 1.0) || max_results < 0)
+        return fail(h, CP_E_ARG, "cp_autotune: bad arguments");
+    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_autotune: the plain kernel has one launch shape");
+    if (path == CP_TUNE_ASSEMBLE && h->n_cells == 0) return fail(h, CP_E_STATE, "cp_autotune: no mesh bound");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, path == CP_TUNE_UPDATE)) return rc;
+    if (path == CP_TUNE_ASSEMBLE && !h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
+        return fail(h, CP_E_NOMEM, "cp_autotune: staging allocation failed");
+    constexpr int V = U2_VARIANTS;
+    std::vector<cudaEvent_t> ev(2 * V * reps, nullptr);
+    for (auto& e : ev) CK(h, cudaEventCreate(&e));
+    const FromArray fa{d_in};
+    const FromMesh fm{d_in, h->d_gradN, h->d_JxW, h->uniform};
+    int rc = CP_OK;
+    const int ng = (int)h->groups.size();
+    for (int gi = 0; gi < ng && rc == CP_OK; ++gi) {
+        Group& g = h->groups[gi];
+        const int64_t m = g.count;
+        auto launch = [&](int v) {
+            return path == CP_TUNE_UPDATE
+                       ? launch_update2(h, g, fa, 0, m, 1, 0.0, 0.0, h->d_P, nullptr, h->d_dPdF, nullptr, h->d_status,
+                                        nullptr, nullptr, v)
+                       : launch_update2(h, g, fm, 0, m, 1, 0.0, 0.0, nullptr, nullptr, nullptr, h->d_stage,
+                                        h->d_status, nullptr, nullptr, v);
+        };
+        if (path == CP_TUNE_UPDATE)
+            sort_group(h, g, fa, 0, m);
+        else
+            sort_group(h, g, fm, 0, m);
+        std::vector<double> ms(V * reps, -1.0);
+        for (int v = 0; v < V && rc == CP_OK; ++v) {
+            cudaError_t e = launch(v);  // untimed first launch
+            for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+                cudaEventRecord(ev[2 * (v * reps + r)], h->stream);
+                e = launch(v);
+                cudaEventRecord(ev[2 * (v * reps + r) + 1], h->stream);
+            }
+            if (e != cudaSuccess) rc = cuda_fail(h, e, "cp_autotune: launch");
+        }
+        if (rc == CP_OK) {
+            const cudaError_t e = cudaStreamSynchronize(h->stream);
+            if (e != cudaSuccess) rc = cuda_fail(h, e, "cp_autotune: synchronize");
+        }
+        if (rc != CP_OK) break;
+        for (int t = 0; t < V * reps; ++t) {
+            float x = 0.f;
+            if (cudaEventElapsedTime(&x, ev[2 * t], ev[2 * t + 1]) == cudaSuccess) ms[t] = x;
+        }
+        const int pmax = g.nt_class == 16 ? 16 : (g.nt_class == 32 ? 32 : 48);
+        const int def = u2_default_variant(pmax, m);
+        const int chosen = cp_tune_select(V, reps, ms.data(), def, min_gain);
+        if (chosen >= 0) g.tuned[path] = chosen;
+        if (results && gi < max_results) {
+            cp_tune_result_t& out = results[gi];
+            out.lattice = g.lattice;
+            out.chosen = chosen;
+            out.default_variant = def;
+            out.reserved = 0;
+            out.n_qp = m;
+            for (int v = 0; v < V; ++v) {
+                std::vector<double> one(ms.begin() + v * reps, ms.begin() + (v + 1) * reps);
+                std::sort(one.begin(), one.end());
+                out.median_ms[v] = one.size() % 2 ? one[one.size() / 2]
+                                                  : 0.5 * (one[one.size() / 2 - 1] + one[one.size() / 2]);
+            }
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    ++h->tune_epoch;
+    return rc == CP_OK ? ng : rc;
+}
+
+int cp_graph_stats(cp_handle* h, int64_t* captures, int64_t* launches) {
+    if (!h) return CP_E_ARG;
+    if (captures) *captures = h->graph_captures;
+    if (launches) *launches = h->graph_launches;
+    return CP_OK;
+}
+
 }  // extern "C"
+

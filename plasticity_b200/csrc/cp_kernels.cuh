@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(QP_BLOCK) classify_kernel(const LatDev* __rest
     if (threadIdx.x < SORT_BUCKETS && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
 }
 
+#ifndef CP_TEMPLATES_ONLY  // the non-template kernels are defined in cp_api.cu
 // exclusive scan of the bucket counts (one warp, SORT_BUCKETS = 64)
 __global__ void bucket_scan_kernel(const int* __restrict__ hist, int* __restrict__ offs) {
     if (threadIdx.x == 0) {
@@ -224,6 +225,8 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
     if (i < i0 + m) perm[base[b] + r] = (int)i;
 }
 
+#endif
+
 // calculatePlasticity over m qps of one group in sorted order (thread j runs
 // internal qp perm[j]).  Outputs by caller index k: P/T/dPdF/status/stats; with a
 // non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
@@ -231,33 +234,9 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
 // size): consecutive threads, and so the lanes of a warp, run solves of
 // similar size.  (Interleaving large- and small-solve warps across SMs,
 // sorting only inside 256-qp blocks, and a persistent grid-stride launch with
-// 64-256 resident threads per SM all measured slower.)
-// Launch shape of the update per lattice class: 256-thread blocks; the FCC
-// class (PMAX 16) at 1 block/SM and up to 255 registers, which measured best
-// (168 registers with 128- or 192-thread blocks measured slower).
-#ifndef CP_U2_SMALL_BLOCK
-#define CP_U2_SMALL_BLOCK 256
-#endif
-#ifndef CP_U2_SMALL_MINB
-#define CP_U2_SMALL_MINB 1
-#endif
-// threads per block of the update for a lattice class (PMAX)
-constexpr int update2_block(int pmax) { return pmax <= 16 ? CP_U2_SMALL_BLOCK : 256; }
-// Resident blocks per SM the compiler sizes registers for: 1 (up to 255
-// registers) for the small FCC-class solve, 2 (128 registers, twice the warps
-// to hide local-memory latency, more spills) for the BCC/HCP classes, whose
-// longer solves gain more from the extra warps than they lose to the spills
-// (measured per class).
-constexpr int update2_min_blocks(int pmax) { return pmax <= 16 ? CP_U2_SMALL_MINB : 2; }
-// Launches of at most UPDATE2_SPREAD_QPS qps (an RVE's or a served request's
-// group) use 64-thread blocks instead, the same registers per thread: one block
-// on each of up to 148 SMs, so each qp's thread shares its SM's L1 with fewer
-// others (measured on the 8^3 RVE: 0.259 -> 0.247 s per solve; on the 2^21-qp
-// batch the 256-thread blocks stay faster).
-constexpr int UPDATE2_SPREAD_BLOCK = 64;
-constexpr int64_t UPDATE2_SPREAD_QPS = 148 * UPDATE2_SPREAD_BLOCK;
-constexpr int update2_spread_min_blocks(int pmax) { return pmax <= 16 ? 4 : 8; }
-
+// 64-256 resident threads per SM all measured slower.)  The launch shape
+// (threads per block, registers per thread) is a template choice, see
+// kU2Shapes in cp_launch.h.
 template <int PMAX, class FSrc>
 __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, const GroupDev& g, const FSrc& fs,
                                             int64_t i, int flag, double F_e, double F_r, double* __restrict__ P,
@@ -295,7 +274,7 @@ __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, cons
     if (status) status[k] = st;
 }
 
-template <int PMAX, class FSrc, int BLOCK = update2_block(PMAX), int MINB = update2_min_blocks(PMAX)>
+template <int PMAX, class FSrc, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
     update2_kernel(const LatDev* __restrict__ L, Opts o, GroupDev g, FSrc fs, const int* __restrict__ perm, int64_t m,
                    int flag, double F_e, double F_r, double* __restrict__ P, double* __restrict__ T, double* __restrict__ dPdF,
@@ -309,6 +288,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                           lattice_id, sD2 + threadIdx.x, BLOCK);
 }
 
+#ifndef CP_TEMPLATES_ONLY
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P
 // and JxW*dP/dF of the cell's 8 qps: thread (cell, node a) writes rows
 // 3a..3a+2 of Ke and Re.  Cells [cell_begin, cell_end) in caller order;
@@ -366,6 +346,8 @@ __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const doub
 #pragma unroll
     for (int r = 0; r < 3; ++r) Re[cell * 24 + 3 * a1 + r] = Rl[r];
 }
+
+#endif
 
 // history initialisation (init.cc:198-330)
 __global__ void init_state_kernel(const LatDev* __restrict__ L, GroupDev g, const double* __restrict__ rod);

@@ -1,0 +1,81 @@
+// cp_launch.h -- host-side launchers of the per-qp kernels.
+//
+// The large per-qp kernels are compiled in their own translation units (one
+// per lattice class, F source and launch shape; plasticity_b200/build.py
+// compiles them in parallel) and reached from cp_api.cu through these
+// launchers, which take plain arguments only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cp_qp.cuh"
+
+namespace cp {
+
+struct FromArray;
+struct FromMesh;
+
+// Arguments of one sorted-update launch over m qps of a lattice group
+// (thread j runs internal qp perm[j]); see update2_kernel.
+struct U2Args {
+    const LatDev* L;
+    Opts o;
+    GroupDev g;
+    const int* perm;
+    int64_t m;
+    int flag;
+    double F_e, F_r;
+    double *P, *T, *dPdF, *stage;
+    int32_t *status, *stats;
+    double *keepF, *keepT;
+    int lattice_id;
+};
+
+// Launch shapes of the sorted update (the autotuner's choices): threads per
+// block and the resident blocks per SM the registers are sized for
+// (__launch_bounds__(block, min_blocks): 255 registers for 256 threads per
+// SM, 128 for 512).
+struct U2Shape {
+    int block, min_blocks;
+};
+constexpr int U2_VARIANTS = 4;
+constexpr U2Shape kU2Shapes[U2_VARIANTS] = {{256, 1}, {256, 2}, {64, 4}, {64, 8}};
+
+// Default shape without tuning: launches of at most U2_SPREAD_QPS qps (an
+// RVE's or a served request's group) in 64-thread blocks spread over the SMs,
+// larger ones in 256-thread blocks; 255 registers for the FCC class (PMAX 16),
+// 128 for the BCC/HCP classes (measured per class).
+constexpr int64_t U2_SPREAD_QPS = 148 * 64;
+inline int u2_default_variant(int pmax, int64_t m) {
+    const bool small_class = pmax <= 16;
+    if (m <= U2_SPREAD_QPS) return small_class ? 2 : 3;
+    return small_class ? 0 : 1;
+}
+
+// Sorted update, one translation unit per (PMAX, F source, variant).
+template <int PMAX, class FSrc, int V>
+cudaError_t launch_update2_v(cudaStream_t s, const U2Args& a, const FSrc& fs);
+
+// Plain thread-per-qp update (F from a caller array) and plain fused assembly
+// of one group, one translation unit per lattice class.
+template <int NT, int PMAX>
+cudaError_t launch_update_plain(cudaStream_t s, const LatDev* L, const Opts& o, const GroupDev& g, const double* F,
+                                int flag, double F_e, double F_r, double* P, double* T, double* dPdF,
+                                int32_t* status, int32_t* stats, double* keepF, double* keepT, int lattice_id);
+template <int NT, int PMAX>
+cudaError_t launch_assemble_plain(cudaStream_t s, const LatDev* L, const Opts& o, const GroupDev& g,
+                                  const double* U, const double* gradN, const double* JxW, int uniform, double F_e,
+                                  double F_r, double* Ke, double* Re, int32_t* status, int32_t* stats,
+                                  int lattice_id);
+
+// Split-BF16 tensor-core contraction of the staged JxW dP/dF of cells
+// [cell_begin, cell_end) into FP32 Ke and, from the staged JxW P, FP64 Re
+// (cp_tc.cu).  gradN: the shared shape-function gradients of a uniform mesh.
+// *err is raised if a wait of the kernel expired.  prepare_ke_tc sets the
+// kernel's shared-memory size once per device.
+cudaError_t prepare_ke_tc();
+cudaError_t launch_ke_tc(cudaStream_t s, const double* stage, const double* gradN, int64_t cell_begin,
+                         int64_t cell_end, float* Ke, double* Re, int* err, int num_sms);
+
+}  // namespace cp

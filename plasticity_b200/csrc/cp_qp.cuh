@@ -5,9 +5,11 @@
 // and inactiveSlipRemoval.cc:4-124 with these restatements (same math,
 // different operation order):
 //   * Schmid tensors are never stored for all systems: resolved shears are
-//     m . (R^T X R) . n with the lattice's crystal-frame m, n; sample-frame
-//     Schmid tensors S = (R m)(R n)^T are formed only for the potentially
-//     active systems.
+//     m . (R^T X R) . n with the lattice's crystal-frame m, n; the
+//     potentially active systems keep S = (R m)(R n)^T as its two vectors and
+//     S : X is formed as (R m) . X (R n).  The sorted kernel (cp_qp2.cuh)
+//     forms every product in the same order, so the two kernels give the
+//     same bits.
 //   * Only the A[PA,PA] block of the consistency matrix is built (the only
 //     block inactive_slip_removal reads, inactiveSlipRemoval.cc:16-24), with
 //     the j-dependent factor hoisted out of the i loop (:273-306).
@@ -103,20 +105,29 @@ __host__ __device__ __forceinline__ double resolved(const LatDev& L, int s, cons
     return m0 * y0 + m1 * y1 + m2 * y2;
 }
 
-// sample-frame Schmid tensor S = (R m)(R n)^T
-__host__ __device__ __forceinline__ M3 schmid(const LatDev& L, int s, const M3& R) {
-    double rm[3], rn[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        rm[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
-        rn[i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
-    }
+// S : X = (R m)^T X (R n) for a Schmid tensor stored as its two vectors
+// v = (R m, R n); the one product form both update kernels use, so that the
+// plain and the sorted kernel round alike
+__host__ __device__ __forceinline__ double schmid_dot(const double* v, const M3& X) {
+    const double y0 = X(0, 0) * v[3] + X(0, 1) * v[4] + X(0, 2) * v[5];
+    const double y1 = X(1, 0) * v[3] + X(1, 1) * v[4] + X(1, 2) * v[5];
+    const double y2 = X(2, 0) * v[3] + X(2, 1) * v[4] + X(2, 2) * v[5];
+    return v[0] * y0 + v[1] * y1 + v[2] * y2;
+}
+__host__ __device__ __forceinline__ M3 schmid_of(const double* v) {
     M3 S;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) S(i, j) = rm[i] * rn[j];
+        for (int j = 0; j < 3; ++j) S(i, j) = v[i] * v[3 + j];
     return S;
+}
+__host__ __device__ __forceinline__ void schmid_vectors(const LatDev& L, int s, const M3& R, double* v) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        v[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
+        v[3 + i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
+    }
 }
 
 // matrixExponential (matrixOperations.cc:165-186)
@@ -223,7 +234,7 @@ struct QpScratch {
     double A[PMAX * PMAX];
     double Apa[PMAX * PMAX];
     double rhs[PMAX * 9];
-    double Spa[PMAX * 9];
+    double Sv[PMAX * 6];  // Schmid tensor of PA system k as its vectors R m, R n
     unsigned char pa[NT], pa0[NT], cur[NT];
 };
 
@@ -322,26 +333,20 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
         for (int k = 0; k < p_init; ++k) {
             const int a = w.pa[k];
             w.h[k] = ldg(&L.h0[a]) * pow((1 - w.s[a] / ldg(&L.ss[a])), ldg(&L.a[a]));
+            schmid_vectors(L, a, R, w.Sv + 6 * k);
         }
         for (int kj = 0; kj < p_init; ++kj) {
             const int bsys = w.pa[kj];
-            const M3 Sj = schmid(L, bsys, R);
+            const M3 Sj = schmid_of(w.Sv + 6 * kj);
             const M3 Y = sym(mul(CE_tr, Sj));
             M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
             axpy(Mj, 2.0, mul(Y, Tst_tr));
             const double dj = w.tau_tr[bsys] - w.W[bsys];
-            for (int c = 0; c < 9; ++c) w.Spa[kj * 9 + c] = Sj.a[c];  // S of PA system kj
-            // column kj of A; rows use S_i . Mj
+            // column kj of A; rows use S_i : Mj
             for (int ki = 0; ki < p_init; ++ki) {
                 const int asys = w.pa[ki];
-                M3 Si;
-                if (ki == kj) {
-                    Si = Sj;
-                } else {
-                    Si = schmid(L, asys, R);
-                }
                 const double di = w.tau_tr[asys] - w.W[asys];
-                const double sm = dot9(Si, Mj);
+                const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
                 double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
                 v += (di * dj < 0.0) ? -sm : sm;
                 const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * w.W[asys];
@@ -402,10 +407,7 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
                 if (w.x_old[k] == 0.0) continue;
                 const int a = w.pa0[k];
                 const double sgn = ((w.tau_tr[a] - w.W[a]) > 0) ? w.x_old[k] : -w.x_old[k];
-                M3 Sa;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) Sa.a[c] = w.Spa[k * 9 + c];
-                axpy(del_FP, sgn, Sa);
+                axpy(del_FP, sgn, schmid_of(w.Sv + 6 * k));
             }
             FP_tau = mul(matexp(del_FP, &e_terms, &status), FP_t2);
             // (:361-396)
@@ -511,10 +513,7 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
                 axpy(dtau, 2.0, mul(dE, Tst));
                 for (int r = 0; r < p; ++r) {
                     const int k = act[r];
-                    M3 Sk;
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) Sk.a[c] = w.Spa[k * 9 + c];
-                    double v = dot9(Sk, dtau);
+                    double v = schmid_dot(w.Sv + 6 * k, dtau);
                     if (neg_t_bits >> w.pa0[k] & 1ull) v = -v;
                     w.rhs[r * 9 + kl] = v;
                 }
@@ -543,9 +542,7 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
             for (int cj = 0; cj < p; ++cj) {
                 const int kj = act[cj];
                 const int bsys = w.pa0[kj];
-                M3 Sj;
-#pragma unroll
-                for (int c = 0; c < 9; ++c) Sj.a[c] = w.Spa[kj * 9 + c];
+                const M3 Sj = schmid_of(w.Sv + 6 * kj);
                 M3 dm, dp;
                 gateaux_pair(Sj, del_FP, c_terms, dm, dp);
                 const M3 Y = sym(mulTN(dm, X6));
@@ -555,11 +552,8 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
                 for (int ci = 0; ci < p; ++ci) {
                     const int ki = act[ci];
                     const int asys = w.pa0[ki];
-                    M3 Si;
-#pragma unroll
-                    for (int c = 0; c < 9; ++c) Si.a[c] = w.Spa[ki * 9 + c];
                     const bool ni = (neg_t_bits >> asys) & 1ull;
-                    const double sm = dot9(Si, Mj);
+                    const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
                     double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
                     v += (ni ^ nj) ? -sm : sm;
                     const double kin = ldg(&L.C1[asys]) - ldg(&L.C2[asys]) * w.W[asys];

@@ -36,29 +36,6 @@ struct Scratch2 {
     double* rhs;  // right-hand sides, 9 per row
 };
 
-// S : X = (R m)^T X (R n) for a Schmid tensor stored as its two vectors
-__host__ __device__ __forceinline__ double schmid_dot(const double* v, const M3& X) {
-    const double y0 = X(0, 0) * v[3] + X(0, 1) * v[4] + X(0, 2) * v[5];
-    const double y1 = X(1, 0) * v[3] + X(1, 1) * v[4] + X(1, 2) * v[5];
-    const double y2 = X(2, 0) * v[3] + X(2, 1) * v[4] + X(2, 2) * v[5];
-    return v[0] * y0 + v[1] * y1 + v[2] * y2;
-}
-__host__ __device__ __forceinline__ M3 schmid_of(const double* v) {
-    M3 S;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) S(i, j) = v[i] * v[3 + j];
-    return S;
-}
-__host__ __device__ __forceinline__ void schmid_vectors(const LatDev& L, int s, const M3& R, double* v) {
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        v[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
-        v[3 + i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
-    }
-}
-
 // a_i[c] -= f a_j[c] for c in [c0, m) on two distinct rows of one matrix.
 // Four columns per step, all loads before the stores: with rows of one array
 // the compiler must otherwise assume a store may feed the next load and runs

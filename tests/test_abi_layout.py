@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OUT = os.path.join(ROOT, "tests", "kernel_emu", "_build")
 
 STRUCTS = {"cp_material_t": capi.CpMaterial, "cp_options_t": capi.CpOptions, "cp_solver_t": capi.CpSolver,
-           "cp_solve_info_t": capi.CpSolveInfo}
+           "cp_solve_info_t": capi.CpSolveInfo, "cp_tune_result_t": capi.CpTuneResult}
 
 
 @pytest.fixture(scope="module")
