@@ -317,10 +317,14 @@ typedef struct cp_solver_t {
                                (cp_assemble_mixed: FP32 Ke, FP64 Re), K scattered to FP32, and the
                                solve as FP64 iterative refinement (r = b - K x in FP64 products of
                                K's FP32 values, stopped at ||r|| <= rel_tolerance ||b||) around
-                               FP32 Jacobi BiCG inner solves to a relative residual of 1e-5
-                               (max_iterations each); BiCG + Jacobi and the true-residual test
-                               only; needs a uniform mesh */
+                               FP32 Jacobi BiCG inner solves to a relative residual of
+                               inner_tolerance (at most 2000 iterations each); a pass is kept when
+                               it cuts ||r|| ten-fold, and the first FP32 pass that does not hands
+                               the remaining passes to FP64 BiCG on the same matrix; BiCG + Jacobi
+                               and the true-residual test only; needs a uniform mesh */
     int32_t max_refinements; /* CP_PRECISION_MIXED: outer refinement passes (0: 10) */
+    double inner_tolerance;  /* CP_PRECISION_MIXED: relative residual of each FP32 inner solve
+                               (0: 1e-5) */
 } cp_solver_t;
 #define CP_PRECISION_FP64 0
 #define CP_PRECISION_MIXED 1
@@ -333,6 +337,10 @@ typedef struct cp_solve_info_t {
     int32_t refinements; /* mixed precision: refinement passes run (0 in FP64) */
     double rhs_norm;      /* ||b|| of the condensed system */
     double residual_norm; /* the tested residual norm at exit */
+    int32_t fp64_iterations; /* of 'iterations', those run in FP64 (all of them in FP64 mode; in
+                               mixed precision the FP64 passes that follow an FP32 pass which
+                               did not cut the residual ten-fold) */
+    int32_t reserved;
 } cp_solve_info_t;
 int cp_solver_default(cp_solver_t* solver); /* BiCG, Jacobi, 50000, 1e-10, true residual */
 

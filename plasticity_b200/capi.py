@@ -97,6 +97,7 @@ class CpSolver(C.Structure):
         ("kernel_mode", C.c_int32),
         ("precision", C.c_int32),
         ("max_refinements", C.c_int32),
+        ("inner_tolerance", C.c_double),
     ]
 
 
@@ -108,6 +109,8 @@ class CpSolveInfo(C.Structure):
         ("refinements", C.c_int32),
         ("rhs_norm", C.c_double),
         ("residual_norm", C.c_double),
+        ("fp64_iterations", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -393,7 +396,8 @@ class CpHandle:
                                                  C.byref(solver) if solver is not None else None,
                                                  C.byref(info)), "cp_newton_iteration")
         return {"iterations": info.iterations, "converged": bool(info.converged), "breakdown": bool(info.breakdown),
-                "refinements": info.refinements, "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
+                "refinements": info.refinements, "fp64_iterations": info.fp64_iterations,
+                "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
 
     def update_from_displacement(self, F_e: float = 0.0, F_r: float = 0.0):
         self._check(self.lib.cp_update_from_displacement(self.h, F_e, F_r), "cp_update_from_displacement")

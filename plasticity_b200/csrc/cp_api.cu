@@ -14,7 +14,7 @@
 #include "../../include/cp_gpu.h"
 #include "cp_kernels.cuh"
 #include "cp_launch.h"
-#include "cp_solve.cuh"
+#include "cp_solve32.cuh"
 
 using namespace cp;
 
@@ -344,6 +344,8 @@ struct cp_handle {
         int64_t n_blocks = 0;                   // node blocks (0: unavailable)
         int64_t *d_blk = nullptr, *d_blkpos = nullptr;  // 3 dofs / 9 entry positions per node block
         double* d_binv = nullptr;               // inverted 3x3 blocks (per solve)
+        float *d_vals32 = nullptr, *d_valsT32 = nullptr;  // mixed precision: K, K^T values (FP32)
+        float* d_vec32 = nullptr;               // mixed precision: MV_COUNT FP32 vectors of n_dofs
         double* d_vec = nullptr;                // n_dofs x SYS_VECS vectors
         double *d_sc = nullptr, *d_partial = nullptr;
         double* d_fpartial = nullptr;           // per-block partials of the fused iteration (n_dofs / 8 + 64)
@@ -489,6 +491,9 @@ void free_system(cp_handle* h) {
     cudaFree(y.d_blk);
     cudaFree(y.d_blkpos);
     cudaFree(y.d_binv);
+    cudaFree(y.d_vals32);
+    cudaFree(y.d_valsT32);
+    cudaFree(y.d_vec32);
     cudaFree(y.d_Ke);
     cudaFree(y.d_Re);
     cudaFree(y.d_Ul);
@@ -1851,17 +1856,7 @@ bool ensure_solve_graphs(cp_handle* h, const cp_solver_t& sv, int every) {
 
 }  // namespace
 
-int cp_solver_default(cp_solver_t* sv) {
-    if (!sv) return CP_E_ARG;
-    sv->kind = CP_SOLVER_BICG;
-    sv->max_iterations = 50000;
-    sv->rel_tolerance = 1.0e-10;
-    sv->precond_norm = 0;
-    sv->check_every = 8;
-    sv->precond = CP_PRECOND_JACOBI;
-    sv->kernel_mode = 0;
-    return CP_OK;
-}
+namespace {
 
 // SpMV units (nodes or rows) per block of the persistent solve's grid: one per
 // warp keeps the dependent column / vector loads of the SpMV short
@@ -1869,77 +1864,37 @@ int cp_solver_default(cp_solver_t* sv) {
 #define CP_PBICG_UNITS_PER_BLOCK 8
 #endif
 
-int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
-                        const cp_solver_t* solver, cp_solve_info_t* info) {
-    if (!h) return CP_E_ARG;
+// Krylov solve of the condensed system K x = rhs (FP64 values in s.d_vals,
+// K^T's in s.d_valsT, the Jacobi diagonal in V_DINV) from x = 0 into V_X:
+// one cooperative launch for small Jacobi BiCG systems, else four kernels
+// per iteration replayed as graphs; hinfo = {iterations, converged,
+// breakdown}, *bnorm_out = ||rhs||
+int krylov_solve(cp_handle* h, const cp_solver_t& sv, const double* rhs, int hinfo[3], double* bnorm_out) {
     auto& s = h->sys;
-    if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_newton_iteration: no dofs bound");
-    cp_solver_t sv;
-    if (solver)
-        sv = *solver;
-    else
-        cp_solver_default(&sv);
-    if ((sv.kind != CP_SOLVER_BICG && sv.kind != CP_SOLVER_BICGSTAB) || sv.max_iterations < 1 ||
-        !(sv.rel_tolerance >= 0.0))
-        return fail(h, CP_E_ARG, "cp_newton_iteration: bad solver settings");
-    if (sv.precond != CP_PRECOND_JACOBI && sv.precond != CP_PRECOND_NODE_BLOCK)
-        return fail(h, CP_E_ARG, "cp_newton_iteration: unknown preconditioner");
-    if (sv.kernel_mode < 0 || sv.kernel_mode > 2) return fail(h, CP_E_ARG, "cp_newton_iteration: bad kernel_mode");
-    if (sv.precond == CP_PRECOND_NODE_BLOCK && (sv.kind != CP_SOLVER_BICG || sv.precond_norm))
-        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: node blocks need BiCG with the true-residual test");
-    if (sv.precond == CP_PRECOND_NODE_BLOCK && !s.n_blocks)
-        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: the dof map has no node blocks");
-    if (int rc = check_device(h)) return rc;
-    if (int rc = ensure_staging(h, false)) return rc;
-    const int64_t n = s.n_dofs, nc = h->n_cells;
+    const int64_t n = s.n_dofs;
     double* V = s.d_vec;
     auto v = [&](int k) { return V + (int64_t)k * n; };
     const unsigned nb = blocks_for(n, SOLVE_BLOCK);
-    // batched getElementalValues at the current u
-    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(v(V_U), s.d_cell_dofs,
-                                                                                         24 * nc, s.d_Ul);
-    if (int rc = cp_assemble_device(h, s.d_Ul, F_e, F_r, s.d_Ke, s.d_Re, h->d_status)) return rc;
-    // K and R (distribute_local_to_global), in cell order per entry
-    scatter_sum_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_Ke, s.d_kptr, s.d_kidx,
-                                                                                     s.nnz, s.d_vals);
-    scatter_sum_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_Re, s.d_rptr, s.d_ridx, n, v(V_R));
-    // condensation of the prescribed increments
-    if (s.n_con && h_du_constrained)
-        CK(h, cudaMemcpyAsync(s.d_duc, h_du_constrained, sizeof(double) * s.n_con, cudaMemcpyHostToDevice,
-                              h->stream));
-    const double* duc = (s.n_con && h_du_constrained) ? s.d_duc : nullptr;
-    CK(h, cudaMemsetAsync(v(V_DC), 0, sizeof(double) * n, h->stream));
-    if (s.n_con)
-        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
-                                                                                                  s.n_con, v(V_DC));
-    sys_spmv(h, v(V_DC), v(V_KDC), nullptr);
-    condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
-    condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
-    jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
-    if (sv.precond == CP_PRECOND_NODE_BLOCK)
-        block_setup_kernel<<<blocks_for(s.n_blocks, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_blkpos,
-                                                                                             s.n_blocks, s.d_binv);
-    transpose_values_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_tpos, s.nnz,
-                                                                                          s.d_valsT);
     // Krylov solve from x = 0: r = r~ = rhs
     CK(h, cudaMemsetAsync(v(V_X), 0, sizeof(double) * n, h->stream));
-    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(V_RES));
-    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(V_RT));
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(rhs, n, v(V_RES));
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(rhs, n, v(V_RT));
     CK(h, cudaMemsetAsync(s.d_done, 0, sizeof(int), h->stream));
     CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
     CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
     CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 8, h->stream));
-    sys_dot(h, v(V_RHS), v(V_RHS), SC_BB, nullptr);
-    sys_dot(h, v(V_RHS), v(V_RHS), SC_RR, nullptr);
+    sys_dot(h, rhs, rhs, SC_BB, nullptr);
+    sys_dot(h, rhs, rhs, SC_RR, nullptr);
     if (sv.precond_norm) {
-        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), v(V_DINV), n, v(V_Z), nullptr);
+        scale_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(rhs, v(V_DINV), n, v(V_Z), nullptr);
         sys_dot(h, v(V_Z), v(V_Z), SC_ZZ, nullptr);
     }
     double sc0[SC_COUNT];
     CK(h, cudaMemcpyAsync(sc0, s.d_sc, sizeof sc0, cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
-    int hinfo[3] = {0, 0, 0};
+    hinfo[0] = hinfo[1] = hinfo[2] = 0;
     const double bnorm = std::sqrt(sc0[SC_BB]);
+    *bnorm_out = bnorm;
     // one cooperative launch for the whole Jacobi BiCG solve (small systems,
     // or on request) where the device can run one
     bool persistent = sv.kind == CP_SOLVER_BICG && sv.precond == CP_PRECOND_JACOBI && sv.kernel_mode != 1 &&
@@ -1972,7 +1927,7 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         CK(h, cudaLaunchCooperativeKernel((const void*)pbicg_kernel, dim3(p_grid), dim3(SOLVE_BLOCK), kargs, 0,
                                           h->stream));
         unsigned tk[8];
-        CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof hinfo, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof(int) * 3, cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaMemcpyAsync(tk, s.d_ticket, sizeof tk, cudaMemcpyDeviceToHost, h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
         if (tk[6]) return fail(h, CP_E_CUDA, "cp_newton_iteration: a grid barrier of the solve timed out");
@@ -1988,11 +1943,262 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
                 for (int t = 0; t < k; ++t) krylov_iteration(h, sv, queued + t == 0);
             queued += k;
             CK(h, cudaGetLastError());
-            CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof hinfo, cudaMemcpyDeviceToHost, h->stream));
+            CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof(int) * 3, cudaMemcpyDeviceToHost, h->stream));
             CK(h, cudaStreamSynchronize(h->stream));
             if (hinfo[1] || hinfo[2]) break;
         }
     }
+    return CP_OK;
+}
+
+// FP32 vectors of the mixed-precision inner solve
+enum MixVec { MV_R = 0, MV_RT, MV_Z, MV_ZT, MV_P, MV_PT, MV_Q, MV_QT, MV_D, MV_DINV, MV_COUNT };
+constexpr double MIXED_INNER_TOL = 1e-5;  // default relative residual of an inner FP32 solve
+constexpr int MIXED_INNER_CAP = 2000;      // iterations of one FP32 pass at most
+
+// One Newton iteration with the mixed-precision assembly and solve
+// (cp_solver_t.precision = CP_PRECISION_MIXED).
+int mixed_newton_iteration(cp_handle* h, const cp_solver_t& sv, const double* h_duc, double F_e, double F_r,
+                           cp_solve_info_t* info) {
+    auto& s = h->sys;
+    const int64_t n = s.n_dofs, nc = h->n_cells;
+    if (!s.d_vals32 &&
+        (cudaMalloc(&s.d_vals32, sizeof(float) * s.nnz) != cudaSuccess ||
+         cudaMalloc(&s.d_valsT32, sizeof(float) * s.nnz) != cudaSuccess ||
+         cudaMalloc(&s.d_vec32, sizeof(float) * MV_COUNT * n) != cudaSuccess))
+        return fail(h, CP_E_NOMEM, "cp_newton_iteration: mixed-precision buffers");
+    double* V = s.d_vec;
+    auto v = [&](int k) { return V + (int64_t)k * n; };
+    auto w = [&](int k) { return s.d_vec32 + (int64_t)k * n; };
+    const unsigned nb = blocks_for(n, SOLVE_BLOCK);
+    float* Ke32 = reinterpret_cast<float*>(s.d_Ke);
+    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(v(V_U), s.d_cell_dofs,
+                                                                                         24 * nc, s.d_Ul);
+    if (int rc = cp_assemble_mixed_device(h, s.d_Ul, F_e, F_r, Ke32, s.d_Re, h->d_status)) return rc;
+    scatter_sum_f32_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(Ke32, s.d_kptr, s.d_kidx,
+                                                                                         s.nnz, s.d_vals32);
+    scatter_sum_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_Re, s.d_rptr, s.d_ridx, n, v(V_R));
+    if (s.n_con && h_duc)
+        CK(h, cudaMemcpyAsync(s.d_duc, h_duc, sizeof(double) * s.n_con, cudaMemcpyHostToDevice, h->stream));
+    const double* duc = (s.n_con && h_duc) ? s.d_duc : nullptr;
+    CK(h, cudaMemsetAsync(v(V_DC), 0, sizeof(double) * n, h->stream));
+    if (s.n_con)
+        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
+                                                                                                  s.n_con, v(V_DC));
+    spmv_f32_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_vals32,
+                                                                                   v(V_DC), n, nullptr, v(V_KDC));
+    condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
+    condense_matrix_f32_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals32);
+    jacobi_setup_f32_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals32, s.d_diag, n, w(MV_DINV));
+    transpose_values_f32_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals32, s.d_tpos,
+                                                                                              s.nnz, s.d_valsT32);
+    // refinement vectors: b in V_RHS; x and r = b - K x in V_PH / V_SH; a
+    // pass's candidate x + d and its residual in V_KDC / V_DC (the roles of
+    // the two pairs swap when a candidate is accepted)
+    int ix = V_PH, ir = V_SH, ixt = V_KDC, irt = V_DC;
+    CK(h, cudaMemsetAsync(v(ix), 0, sizeof(double) * n, h->stream));
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_RHS), n, v(ir));
+    CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 8, h->stream));
+    CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
+    sys_dot(h, v(V_RHS), v(V_RHS), SC_BB, nullptr);
+    double sc0[SC_COUNT];
+    CK(h, cudaMemcpyAsync(sc0, s.d_sc, sizeof sc0, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    CK(h, cudaGetLastError());
+    const double bnorm = std::sqrt(sc0[SC_BB]);
+    double rnorm = bnorm;
+    int total_iters = 0, iters64 = 0, passes = 0, breakdown = 0;
+    bool use64 = false, have64 = false;
+    const int max_passes = sv.max_refinements > 0 ? sv.max_refinements : 10;
+    const int every = sv.check_every > 0 ? sv.check_every : 8;
+    const double tol_in = sv.inner_tolerance > 0.0 ? sv.inner_tolerance : MIXED_INNER_TOL;
+    const int cap32 = std::min(sv.max_iterations, MIXED_INNER_CAP);
+    cp_solver_t sv64 = sv;
+    sv64.precision = CP_PRECISION_FP64;
+    while (bnorm != 0.0 && !(rnorm <= sv.rel_tolerance * bnorm) && passes < max_passes) {
+        ++passes;
+        int hinfo[3] = {0, 0, 0};
+        if (!use64) {
+            // the inner FP32 solve K d = r from d = 0
+            mixed_start_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(ir), n, w(MV_R), w(MV_RT), w(MV_D));
+            CK(h, cudaMemsetAsync(s.d_done, 0, sizeof(int), h->stream));
+            CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
+            CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
+            CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 8, h->stream));
+            norm2_f32_kernel<<<RED_BLOCKS, SOLVE_BLOCK, 0, h->stream>>>(w(MV_R), n, s.d_sc, SC_BB, s.d_fpartial,
+                                                                        s.d_ticket + 3);
+            int queued = 0;
+            const int* done = s.d_done;
+            while (queued < cap32) {
+                const int k = std::min(every, cap32 - queued);
+                for (int t = 0; t < k; ++t) {
+                    mbicg_precond_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(w(MV_DINV), w(MV_R), w(MV_RT), n,
+                                                                            w(MV_Z), w(MV_ZT), s.d_sc, s.d_fpartial,
+                                                                            s.d_ticket + 0, done);
+                    mbicg_dir_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, w(MV_Z), w(MV_ZT), n,
+                                                                        queued + t == 0, w(MV_P), w(MV_PT), s.d_done,
+                                                                        s.d_info);
+                    if (s.triples)
+                        mbicg_spmv3_kernel<<<(int)std::min<int64_t>(blocks_for(32 * (n / 3), SOLVE_BLOCK),
+                                                                    SPMV3_GRID),
+                                             SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_vals32,
+                                                                          s.d_valsT32, w(MV_P), w(MV_PT), n, w(MV_Q),
+                                                                          w(MV_QT), s.d_sc, s.d_fpartial,
+                                                                          s.d_ticket + 1, done);
+                    else
+                        mbicg_spmv_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+                            s.d_row_ptr, s.d_col, s.d_vals32, s.d_valsT32, w(MV_P), w(MV_PT), n, w(MV_Q), w(MV_QT),
+                            s.d_sc, s.d_fpartial, s.d_ticket + 1, done);
+                    mbicg_step_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_sc, w(MV_P), w(MV_Q), w(MV_QT), n,
+                                                                         tol_in, w(MV_D), w(MV_R), w(MV_RT),
+                                                                         s.d_fpartial, s.d_ticket + 2, s.d_done,
+                                                                         s.d_info);
+                }
+                queued += k;
+                CK(h, cudaGetLastError());
+                CK(h, cudaMemcpyAsync(hinfo, s.d_info, sizeof(int) * 3, cudaMemcpyDeviceToHost, h->stream));
+                CK(h, cudaStreamSynchronize(h->stream));
+                if (hinfo[1] || hinfo[2]) break;
+            }
+            total_iters += hinfo[0];
+            if (hinfo[2]) breakdown = 1;
+            mixed_try_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(ix), w(MV_D), nullptr, n, v(ixt));
+        } else {
+            // an FP64 inner solve on the same (FP32-assembled) matrix
+            if (!have64) {
+                promote_f32_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals32, s.nnz,
+                                                                                                s.d_vals);
+                promote_f32_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_valsT32, s.nnz,
+                                                                                                s.d_valsT);
+                jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
+                have64 = true;
+            }
+            double bn = 0.0;
+            if (int rc = krylov_solve(h, sv64, v(ir), hinfo, &bn)) return rc;
+            total_iters += hinfo[0];
+            iters64 += hinfo[0];
+            if (hinfo[2]) breakdown = 1;
+            mixed_try_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(ix), nullptr, v(V_X), n, v(ixt));
+        }
+        // the candidate's residual b - K (x + d) in FP64
+        spmv_f32_kernel<<<blocks_for(32 * n, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+            s.d_row_ptr, s.d_col, s.d_vals32, v(ixt), n, v(V_RHS), v(irt));
+        sys_dot(h, v(irt), v(irt), SC_RR, nullptr);
+        double rr = 0.0;
+        CK(h, cudaMemcpyAsync(&rr, s.d_sc + SC_RR, sizeof rr, cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+        const double rt = std::sqrt(rr);
+        // accepted when it cuts the residual ten-fold (or meets the tolerance);
+        // an FP32 pass that does not hands the rest of the solve to FP64 passes
+        const bool good = std::isfinite(rt) && (rt <= 0.1 * rnorm || rt <= sv.rel_tolerance * bnorm);
+        if (good || (use64 && std::isfinite(rt) && rt < rnorm)) {
+            std::swap(ix, ixt);
+            std::swap(ir, irt);
+            rnorm = rt;
+        } else if (use64) {
+            break;  // the FP64 pass made no progress either
+        }
+        if (!good) use64 = true;
+    }
+    copy_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(ix), n, v(V_X));
+    if (s.n_con)
+        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
+                                                                                                  s.n_con, v(V_X));
+    add_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_X), n, v(V_U));
+    CK(h, cudaGetLastError());
+    if (int rc = check_tc_error(h)) return rc;
+    if (info) {
+        info->iterations = total_iters;
+        info->converged = bnorm == 0.0 || rnorm <= sv.rel_tolerance * bnorm;
+        info->breakdown = breakdown;
+        info->refinements = passes;
+        info->fp64_iterations = iters64;
+        info->rhs_norm = bnorm;
+        info->residual_norm = bnorm == 0.0 ? 0.0 : rnorm;
+    }
+    return CP_OK;
+}
+
+}  // namespace
+
+int cp_solver_default(cp_solver_t* sv) {
+    if (!sv) return CP_E_ARG;
+    sv->kind = CP_SOLVER_BICG;
+    sv->max_iterations = 50000;
+    sv->rel_tolerance = 1.0e-10;
+    sv->precond_norm = 0;
+    sv->check_every = 8;
+    sv->precond = CP_PRECOND_JACOBI;
+    sv->kernel_mode = 0;
+    sv->precision = CP_PRECISION_FP64;
+    sv->max_refinements = 0;
+    sv->inner_tolerance = 0.0;
+    return CP_OK;
+}
+
+
+int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
+                        const cp_solver_t* solver, cp_solve_info_t* info) {
+    if (!h) return CP_E_ARG;
+    auto& s = h->sys;
+    if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_newton_iteration: no dofs bound");
+    cp_solver_t sv;
+    if (solver)
+        sv = *solver;
+    else
+        cp_solver_default(&sv);
+    if ((sv.kind != CP_SOLVER_BICG && sv.kind != CP_SOLVER_BICGSTAB) || sv.max_iterations < 1 ||
+        !(sv.rel_tolerance >= 0.0))
+        return fail(h, CP_E_ARG, "cp_newton_iteration: bad solver settings");
+    if (sv.precond != CP_PRECOND_JACOBI && sv.precond != CP_PRECOND_NODE_BLOCK)
+        return fail(h, CP_E_ARG, "cp_newton_iteration: unknown preconditioner");
+    if (sv.kernel_mode < 0 || sv.kernel_mode > 2) return fail(h, CP_E_ARG, "cp_newton_iteration: bad kernel_mode");
+    if (sv.precond == CP_PRECOND_NODE_BLOCK && (sv.kind != CP_SOLVER_BICG || sv.precond_norm))
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: node blocks need BiCG with the true-residual test");
+    if (sv.precond == CP_PRECOND_NODE_BLOCK && !s.n_blocks)
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: the dof map has no node blocks");
+    if (sv.precision != CP_PRECISION_FP64 && sv.precision != CP_PRECISION_MIXED)
+        return fail(h, CP_E_ARG, "cp_newton_iteration: unknown precision");
+    if (sv.precision == CP_PRECISION_MIXED &&
+        (sv.kind != CP_SOLVER_BICG || sv.precond != CP_PRECOND_JACOBI || sv.precond_norm || sv.max_refinements < 0 ||
+         !(sv.inner_tolerance >= 0.0 && sv.inner_tolerance < 1.0)))
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: mixed precision runs Jacobi BiCG, true residual");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    if (sv.precision == CP_PRECISION_MIXED) return mixed_newton_iteration(h, sv, h_du_constrained, F_e, F_r, info);
+    const int64_t n = s.n_dofs, nc = h->n_cells;
+    double* V = s.d_vec;
+    auto v = [&](int k) { return V + (int64_t)k * n; };
+    const unsigned nb = blocks_for(n, SOLVE_BLOCK);
+    // batched getElementalValues at the current u
+    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(v(V_U), s.d_cell_dofs,
+                                                                                         24 * nc, s.d_Ul);
+    if (int rc = cp_assemble_device(h, s.d_Ul, F_e, F_r, s.d_Ke, s.d_Re, h->d_status)) return rc;
+    // K and R (distribute_local_to_global), in cell order per entry
+    scatter_sum_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_Ke, s.d_kptr, s.d_kidx,
+                                                                                     s.nnz, s.d_vals);
+    scatter_sum_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_Re, s.d_rptr, s.d_ridx, n, v(V_R));
+    // condensation of the prescribed increments
+    if (s.n_con && h_du_constrained)
+        CK(h, cudaMemcpyAsync(s.d_duc, h_du_constrained, sizeof(double) * s.n_con, cudaMemcpyHostToDevice,
+                              h->stream));
+    const double* duc = (s.n_con && h_du_constrained) ? s.d_duc : nullptr;
+    CK(h, cudaMemsetAsync(v(V_DC), 0, sizeof(double) * n, h->stream));
+    if (s.n_con)
+        constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
+                                                                                                  s.n_con, v(V_DC));
+    sys_spmv(h, v(V_DC), v(V_KDC), nullptr);
+    condense_rhs_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(v(V_R), v(V_KDC), v(V_DC), s.d_cmask, n, v(V_RHS));
+    condense_matrix_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_row_ptr, s.d_col, s.d_cmask, n, s.d_vals);
+    jacobi_setup_kernel<<<nb, SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_diag, n, v(V_DINV));
+    if (sv.precond == CP_PRECOND_NODE_BLOCK)
+        block_setup_kernel<<<blocks_for(s.n_blocks, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_blkpos,
+                                                                                             s.n_blocks, s.d_binv);
+    transpose_values_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_vals, s.d_tpos, s.nnz,
+                                                                                          s.d_valsT);
+    int hinfo[3] = {0, 0, 0};
+    double bnorm = 0.0;
+    if (int rc = krylov_solve(h, sv, v(V_RHS), hinfo, &bnorm)) return rc;
     // distribute: constrained dofs take their prescribed increments exactly
     if (s.n_con)
         constrained_vector_kernel<<<blocks_for(s.n_con, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_con, duc,
@@ -2006,6 +2212,8 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         info->iterations = hinfo[0];
         info->converged = hinfo[1];
         info->breakdown = hinfo[2];
+        info->refinements = 0;
+        info->fp64_iterations = hinfo[0];
         info->rhs_norm = bnorm;
         info->residual_norm = bnorm == 0.0 ? 0.0 : std::sqrt(sv.precond_norm ? scf[SC_ZZ] : scf[SC_RR]);
     }
