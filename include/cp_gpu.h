@@ -418,6 +418,9 @@ int cp_synchronize(cp_handle* h);
 int cp_set_timing(cp_handle* h, int32_t enable);
 int cp_get_timing(cp_handle* h, int32_t max_groups, int32_t* lattice, int64_t* count,
                   int64_t* launches, double* total_ms);
+/* The same for the element-contraction launches of the assembly calls:
+ * kind 0 the FP64 contraction, kind 1 the tensor-core one. */
+int cp_get_contract_timing(cp_handle* h, int32_t kind, int64_t* launches, double* total_ms);
 
 /* Diagnostics: measured FP64 FMA throughput of the device (TFLOP/s), the
  * denominator of the FP64 roofline of the qp update (no counterpart in the

@@ -245,6 +245,7 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_measure_fp64_peak": (C.c_int, [C.c_int32, D]),
         "cp_set_timing": (C.c_int, [H, C.c_int32]),
         "cp_get_timing": (C.c_int, [H, C.c_int32, I32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), D]),
+        "cp_get_contract_timing": (C.c_int, [H, C.c_int32, C.POINTER(C.c_int64), D]),
         "cp_autotune": (C.c_int, [H, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(CpTuneResult),
                                   C.c_int32]),
         "cp_tune_select": (C.c_int32, [C.c_int32, C.c_int32, D, C.c_int32, C.c_double]),
@@ -359,6 +360,12 @@ class CpHandle:
                                                dptr(Re), iptr(st)), "cp_assemble_mixed")
         return Ke, Re, st
 
+    def assemble_mixed_device(self, U_ptr, F_e, F_r, Ke_ptr, Re_ptr, status_ptr=None):
+        self._check(self.lib.cp_assemble_mixed_device(self.h, C.c_void_p(U_ptr), F_e, F_r, C.c_void_p(Ke_ptr),
+                                                      C.c_void_p(Re_ptr),
+                                                      C.c_void_p(status_ptr) if status_ptr else None),
+                    "cp_assemble_mixed_device")
+
     def assemble_device(self, U_ptr, F_e, F_r, Ke_ptr, Re_ptr, status_ptr=None):
         self._check(self.lib.cp_assemble_device(self.h, C.c_void_p(U_ptr), F_e, F_r, C.c_void_p(Ke_ptr),
                                                 C.c_void_p(Re_ptr),
@@ -440,6 +447,12 @@ class CpHandle:
             self._check(ng, "cp_autotune")
         return [{"lattice": res[g].lattice, "n_qp": res[g].n_qp, "chosen": res[g].chosen,
                  "default": res[g].default_variant, "median_ms": list(res[g].median_ms)} for g in range(ng)]
+
+    def contract_timing(self, kind: int):
+        """(launches, total ms) of the timed element contractions: kind 0 FP64, 1 tensor-core."""
+        a, b = C.c_int64(), C.c_double()
+        self._check(self.lib.cp_get_contract_timing(self.h, kind, C.byref(a), C.byref(b)), "cp_get_contract_timing")
+        return int(a.value), float(b.value)
 
     def graph_stats(self):
         """(graphs captured, graph launches) since the handle was created."""

@@ -370,6 +370,8 @@ struct cp_handle {
     std::vector<Pending> pending;
     std::vector<double> group_ms;
     std::vector<int64_t> group_launches;
+    double contract_ms[2] = {0.0, 0.0};       // element contractions: [0] FP64, [1] tensor-core
+    int64_t contract_launches[2] = {0, 0};
     // captured calls (cp_options_t.use_graphs): a few graphs keyed by the
     // call's kind, pointers, scalars and launch shapes, least recently used
     // replaced first
@@ -1120,8 +1122,11 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
             for (size_t gi = 0; gi < h->groups.size(); ++gi)
                 sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status,
                                     nullptr, nullptr);
+            cudaEvent_t ev{};
+            timing_begin(h, -1, &ev);
             contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, h->stream>>>(
                 h->d_stage, h->d_gradN, h->uniform, 0, h->n_cells, d_Ke, d_Re);
+            timing_end(h, -1, ev);
             CK(h, cudaGetLastError());
             return CP_OK;
         });
@@ -1239,7 +1244,10 @@ int cp_assemble_mixed_device(cp_handle* h, const double* d_U, double F_e, double
             sorted_update_group(h, gi, fm, 1, F_e, F_r, nullptr, nullptr, nullptr, h->d_stage, d_status, nullptr,
                                 nullptr);
         CK(h, cudaGetLastError());
+        cudaEvent_t ev{};
+        timing_begin(h, -2, &ev);
         CK(h, launch_ke_tc(h->stream, h->d_stage, h->d_gradN, 0, h->n_cells, d_Ke, d_Re, h->d_tc_err, h->num_sms));
+        timing_end(h, -2, ev);
         return CP_OK;
     });
 }
@@ -1508,6 +1516,8 @@ int cp_set_timing(cp_handle* h, int32_t enable) {
     h->timing = enable != 0;
     h->group_ms.assign(h->groups.size(), 0.0);
     h->group_launches.assign(h->groups.size(), 0);
+    h->contract_ms[0] = h->contract_ms[1] = 0.0;
+    h->contract_launches[0] = h->contract_launches[1] = 0;
     return CP_OK;
 }
 
@@ -1523,8 +1533,13 @@ int cp_get_timing(cp_handle* h, int32_t max_groups, int32_t* lattice, int64_t* c
     for (auto& p : h->pending) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, p.a, p.b);
-        h->group_ms[p.group] += ms;
-        h->group_launches[p.group] += 1;
+        if (p.group < 0) {  // -1: FP64 contraction, -2: tensor-core contraction
+            h->contract_ms[-p.group - 1] += ms;
+            h->contract_launches[-p.group - 1] += 1;
+        } else {
+            h->group_ms[p.group] += ms;
+            h->group_launches[p.group] += 1;
+        }
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
     }
@@ -1537,6 +1552,16 @@ int cp_get_timing(cp_handle* h, int32_t max_groups, int32_t* lattice, int64_t* c
         if (total_ms) total_ms[g] = h->group_ms[g];
     }
     return ng;
+}
+
+int cp_get_contract_timing(cp_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
+    if (!h || kind < 0 || kind > 1) return CP_E_ARG;
+    int64_t dummy[CP_MAX_LATTICES];
+    const int ng = cp_get_timing(h, 0, nullptr, dummy, nullptr, nullptr);  // folds the pending events in
+    if (ng < 0) return ng;
+    if (launches) *launches = h->contract_launches[kind];
+    if (total_ms) *total_ms = h->contract_ms[kind];
+    return CP_OK;
 }
 
 int cp_synchronize(cp_handle* h) {
