@@ -242,9 +242,10 @@ int cp_averages(cp_handle* h, double out[22]);
  * Same inputs, outputs and summation order as cp_averages.  Limits and rules:
  *   - at most CP_NOALLOC_AVG_MAX_QPS bound qps; larger handles get CP_E_ARG
  *     with a message naming the limit;
- *   - the first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) for that device; make that first call before
- *     any stream capture;
+ *   - the first call on a handle looks up the array's device address
+ *     (cudaGetSymbolAddress, with the handle's device current) and keeps it
+ *     in the handle; make that first call before any stream capture (the
+ *     address does not survive a device reset, which no handle survives);
  *   - every call on a device shares the one array and it keeps the last
  *     call's contents (each call writes every entry it reads, so nothing
  *     needs clearing); calls that overlap on the GPU (different handles on
@@ -356,6 +357,14 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
                         const cp_solver_t* solver, cp_solve_info_t* info);
 
 /*
+ * The second half of cp_newton_iteration: K and R from the element matrices
+ * already in the handle's system (written by cp_batch_assemble), the
+ * condensation, the Krylov solve, distribute and u += du.  FP64 only.
+ */
+int cp_newton_solve(cp_handle* h, const double* h_du_constrained, const cp_solver_t* solver,
+                    cp_solve_info_t* info);
+
+/*
  * The post-pass calculatePlasticity(...,0) at every qp
  * (updateAfterIncrement.cc:105) with F from the device displacement; then
  * cp_averages / cp_reorient / cp_commit as after cp_update.
@@ -407,6 +416,36 @@ int32_t cp_tune_select(int32_t n_variants, int32_t reps, const double* ms, int32
  * since its creation (cp_options_t.use_graphs). */
 int cp_graph_stats(cp_handle* h, int64_t* captures, int64_t* launches);
 
+/*
+ * Continuous batching of independent requests (served RVE solves; no
+ * counterpart in the reference, which solves one problem per process).  A
+ * cp_batch is a queue on one device on which the calculatePlasticity work of
+ * several handles runs as shared launches: one counting sort over all their
+ * lattice groups and one update launch per lattice class (FCC / BCC / HCP
+ * sized solves) over the qps of every handle, each qp with its own handle's
+ * constants, history and displacement field.  Per-qp arithmetic is that of
+ * the per-handle launches, so results do not depend on what shares a
+ * launch.  The handles need cp_bind_dofs (the displacement u is gathered on
+ * the device) and the sorted update.
+ *   cp_batch_assemble: the Newton iteration's assembly at each handle's u
+ *     (flag 1; Ke/Re into the handle's system); follow it with
+ *     cp_newton_solve on each handle.
+ *   cp_batch_post: the post-pass (flag 0) at each handle's u; follow it with
+ *     cp_averages / cp_reorient / cp_commit as after
+ *     cp_update_from_displacement.
+ * F_e, F_r: n values, each handle's twin-rule scalars.  At most 64 handles'
+ * worth of groups per launch (larger lists run as several).  Asynchronous:
+ * ordered after the work already queued on each handle's stream and before
+ * the work queued there afterwards.
+ */
+typedef struct cp_batch cp_batch;
+int cp_batch_create(int32_t device, cp_batch** out);
+void cp_batch_destroy(cp_batch* b);
+const char* cp_batch_last_error(const cp_batch* b);
+int64_t cp_batch_launches(const cp_batch* b); /* shared update launches issued so far */
+int cp_batch_assemble(cp_batch* b, cp_handle* const* hs, int32_t n, const double* F_e, const double* F_r);
+int cp_batch_post(cp_batch* b, cp_handle* const* hs, int32_t n, const double* F_e, const double* F_r);
+
 /* Wait for all work queued on the handle's stream. */
 int cp_synchronize(cp_handle* h);
 
@@ -426,6 +465,15 @@ int cp_get_contract_timing(cp_handle* h, int32_t kind, int64_t* launches, double
  * denominator of the FP64 roofline of the qp update (no counterpart in the
  * reference). */
 int cp_measure_fp64_peak(int32_t device, double* tflops);
+
+/* Diagnostics: make the next persistent Jacobi BiCG solves (cp_solver_t
+ * kernel_mode 0 on small systems, or 2) wait at most wait_seconds at each
+ * grid barrier (0: the default 1 s) and, with withhold_block >= 0, have that
+ * block of the solve's grid never arrive, so that every wait runs out: the
+ * solve then returns CP_E_CUDA ("a grid barrier of the solve timed out") and
+ * the context stays usable.  (-1, 0) restores the normal solve.  No
+ * counterpart in the reference. */
+int cp_debug_barrier_test(cp_handle* h, int32_t withhold_block, double wait_seconds);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own
  * device work (input uploads, output reads) with the *_device entry points. */

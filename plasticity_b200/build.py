@@ -4,7 +4,8 @@ The product is a plain C-ABI shared library (include/cp_gpu.h); Python loads
 it with ctypes.  Built with nvcc directly, so the .so lives in the source
 tree and travels with it.  The large per-qp kernels are separate translation
 units (one per lattice class, F source and launch shape of the sorted update;
-one per lattice class of the plain kernels) compiled in parallel and linked
+one per lattice class of the plain and the batched kernels) compiled in
+parallel and linked
 into the one library.
 """
 from __future__ import annotations
@@ -42,6 +43,8 @@ def units():
                             [f"-DCP_TU_PMAX={pmax}", f"-DCP_TU_FSRC={fsrc}", f"-DCP_TU_VARIANT={v}"]))
     for nt, pmax in ((16, 16), (32, 32), (64, 48)):
         out.append((f"plain_{nt}", "cp_plain_tu.cu", [f"-DCP_TU_NT={nt}", f"-DCP_TU_PMAX={pmax}"]))
+    for pmax in (16, 32, 48):
+        out.append((f"batch_{pmax}", "cp_batch_tu.cu", [f"-DCP_TU_PMAX={pmax}"]))
     return [u for u in out if os.path.exists(os.path.join(CSRC, u[1]))]
 
 

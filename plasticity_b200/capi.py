@@ -24,6 +24,11 @@ CP_MAX_SYSTEMS = 64
 CP_MAX_LATTICES = 8
 
 CP_OK = 0
+CP_E_ARG = -1
+CP_E_STATE = -2
+CP_E_CUDA = -3
+CP_E_NOMEM = -4
+CP_E_UNSUPPORTED = -5
 CP_QP_NONFINITE = 1
 CP_QP_SINGULAR = 2
 CP_QP_ACTIVE_OVERFLOW = 4
@@ -249,6 +254,14 @@ def load_library(path: str | None = None) -> C.CDLL:
         "cp_autotune": (C.c_int, [H, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(CpTuneResult),
                                   C.c_int32]),
         "cp_tune_select": (C.c_int32, [C.c_int32, C.c_int32, D, C.c_int32, C.c_double]),
+        "cp_debug_barrier_test": (C.c_int, [H, C.c_int32, C.c_double]),
+        "cp_newton_solve": (C.c_int, [H, D, C.POINTER(CpSolver), C.POINTER(CpSolveInfo)]),
+        "cp_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+        "cp_batch_destroy": (None, [C.c_void_p]),
+        "cp_batch_last_error": (C.c_char_p, [C.c_void_p]),
+        "cp_batch_launches": (C.c_int64, [C.c_void_p]),
+        "cp_batch_assemble": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, D, D]),
+        "cp_batch_post": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, D, D]),
         "cp_graph_stats": (C.c_int, [H, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
@@ -406,6 +419,16 @@ class CpHandle:
                 "refinements": info.refinements, "fp64_iterations": info.fp64_iterations,
                 "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
 
+    def newton_solve(self, du_constrained=None, solver: CpSolver | None = None):
+        """cp_newton_solve: the solve half of a Newton pass whose Ke/Re a cp_batch_assemble wrote."""
+        duc = None if du_constrained is None else as_f64(du_constrained)
+        info = CpSolveInfo()
+        self._check(self.lib.cp_newton_solve(self.h, dptr(duc), C.byref(solver) if solver is not None else None,
+                                             C.byref(info)), "cp_newton_solve")
+        return {"iterations": info.iterations, "converged": bool(info.converged), "breakdown": bool(info.breakdown),
+                "refinements": info.refinements, "fp64_iterations": info.fp64_iterations,
+                "rhs_norm": info.rhs_norm, "residual_norm": info.residual_norm}
+
     def update_from_displacement(self, F_e: float = 0.0, F_r: float = 0.0):
         self._check(self.lib.cp_update_from_displacement(self.h, F_e, F_r), "cp_update_from_displacement")
 
@@ -472,3 +495,46 @@ class CpHandle:
         if ng < 0:
             self._check(ng, "cp_get_timing")
         return [(int(lat[g]), int(cnt[g]), int(lau[g]), float(ms[g])) for g in range(ng)]
+
+
+class CpBatch:
+    """A cp_batch queue: the sorted updates of several handles on one device
+    as shared launches (continuous batching of served requests)."""
+
+    def __init__(self, device: int = 0, lib: C.CDLL | None = None):
+        self.lib = lib or load_library()
+        b = C.c_void_p()
+        rc = self.lib.cp_batch_create(device, C.byref(b))
+        if rc != CP_OK:
+            raise CpError(f"cp_batch_create failed ({rc})")
+        self.b = b
+
+    def _run(self, fn, handles, F_e, F_r, what):
+        n = len(handles)
+        hs = (C.c_void_p * n)(*[h.h for h in handles])
+        fe = np.ascontiguousarray(F_e, dtype=np.float64)
+        fr = np.ascontiguousarray(F_r, dtype=np.float64)
+        rc = fn(self.b, hs, n, dptr(fe), dptr(fr))
+        if rc != CP_OK:
+            msg = self.lib.cp_batch_last_error(self.b)
+            raise CpError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def assemble(self, handles, F_e, F_r):
+        self._run(self.lib.cp_batch_assemble, handles, F_e, F_r, "cp_batch_assemble")
+
+    def post(self, handles, F_e, F_r):
+        self._run(self.lib.cp_batch_post, handles, F_e, F_r, "cp_batch_post")
+
+    def launches(self) -> int:
+        return int(self.lib.cp_batch_launches(self.b))
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.cp_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

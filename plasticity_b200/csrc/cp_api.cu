@@ -5,7 +5,6 @@
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
-#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -243,6 +242,62 @@ __global__ void mesh_F_kernel(FromMesh fm, int64_t n_qp, double* __restrict__ F)
     for (int c = 0; c < 9; ++c) F[9 * k + c] = f.a[c];
 }
 
+// ---- the counting sort of several handles' groups (batched launches, see
+// BatchDesc): histogram reset, classification, scan and scatter per group
+__global__ void batch_hist_zero_kernel(const __grid_constant__ BatchArgs a) {
+    if ((int)blockIdx.x < a.n && threadIdx.x < 2 * SORT_BUCKETS) a.d[blockIdx.x].hist[threadIdx.x] = 0;
+}
+
+__global__ void __launch_bounds__(QP_BLOCK) classify_batch_kernel(const __grid_constant__ BatchArgs a) {
+    __shared__ int sh[SORT_BUCKETS];
+    int64_t lb = 0;
+    const int k = batch_group_of_block(a, QP_BLOCK, lb);
+    if (k < 0) return;
+    const BatchDesc& d = a.d[k];
+    if (threadIdx.x < SORT_BUCKETS) sh[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = lb * QP_BLOCK + threadIdx.x;
+    if (i < d.m) {
+        const int p0 = count_potentially_active(*d.L, d.o, d.g, i, d.fm(d.g.qp[i]));
+        const int b = SORT_BUCKETS - 1 - (p0 < SORT_BUCKETS - 1 ? p0 : SORT_BUCKETS - 1);
+        d.key[i] = (unsigned char)b;
+        atomicAdd(&sh[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < SORT_BUCKETS && sh[threadIdx.x]) atomicAdd(&d.hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+__global__ void bucket_scan_batch_kernel(const __grid_constant__ BatchArgs a) {
+    if ((int)blockIdx.x >= a.n || threadIdx.x != 0) return;
+    int* h = a.d[blockIdx.x].hist;
+    int acc = 0;
+    for (int b = 0; b < SORT_BUCKETS; ++b) {
+        h[SORT_BUCKETS + b] = acc;
+        acc += h[b];
+    }
+}
+
+__global__ void __launch_bounds__(256) bucket_scatter_batch_kernel(const __grid_constant__ BatchArgs a) {
+    __shared__ int cnt[SORT_BUCKETS], base[SORT_BUCKETS];
+    int64_t lb = 0;
+    const int k = batch_group_of_block(a, 256, lb);
+    if (k < 0) return;
+    const BatchDesc& d = a.d[k];
+    if (threadIdx.x < SORT_BUCKETS) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t i = lb * 256 + threadIdx.x;
+    int b = 0, r = 0;
+    if (i < d.m) {
+        b = d.key[i];
+        r = atomicAdd(&cnt[b], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < SORT_BUCKETS)
+        base[threadIdx.x] = cnt[threadIdx.x] ? atomicAdd(&d.hist[SORT_BUCKETS + threadIdx.x], cnt[threadIdx.x]) : 0;
+    __syncthreads();
+    if (i < d.m) d.perm[base[b] + r] = (int)i;
+}
+
 // FP64 FMA throughput probe: 8 independent dependent-FMA chains per thread.
 __global__ void fp64_fma_probe_kernel(int iters, double seed, double* out) {
     double a[8];
@@ -361,6 +416,9 @@ struct cp_handle {
     // averages scratch
     double *d_avg_partial = nullptr, *d_avg_out = nullptr;
     int64_t avg_cap = 0;
+    double* noalloc_scratch = nullptr;  // device address of g_noalloc_avg_scratch (cp_averages_noalloc)
+    unsigned long long barrier_wait_ns = 0;  // cp_debug_barrier_test: 0 = the default wait
+    int barrier_withhold = -1;
     // optional per-launch timing of the update/assembly kernels
     bool timing = false;
     struct Pending {
@@ -397,6 +455,17 @@ struct cp_handle {
     uint64_t graph_clock = 0;
     int64_t graph_captures = 0, graph_launches = 0;
     int64_t tune_epoch = 0;  // bumped whenever a group's launch shape changes
+    std::string err;
+};
+
+// A batching queue: one stream on which the sorted updates of several
+// handles run as shared launches (cp_batch_assemble / cp_batch_post).
+struct cp_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_done = nullptr;
+    std::vector<cudaEvent_t> ev_in;
+    int64_t launches = 0;  // batched update launches issued
     std::string err;
 };
 
@@ -1311,26 +1380,6 @@ int cp_averages(cp_handle* h, double out[22]) {
     return CP_OK;
 }
 
-// Device address of g_noalloc_avg_scratch, looked up once per device (the
-// symbol's host-side name is a stand-in, not a device address).
-static double* noalloc_avg_scratch(int device, cudaError_t* err) {
-    static std::mutex mu;
-    static double* addr[64] = {nullptr};
-    *err = cudaSuccess;
-    if (device < 0 || device >= 64) {
-        *err = cudaErrorInvalidDevice;
-        return nullptr;
-    }
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
-        void* p = nullptr;
-        *err = cudaGetSymbolAddress(&p, g_noalloc_avg_scratch);
-        if (*err != cudaSuccess) return nullptr;
-        addr[device] = static_cast<double*>(p);
-    }
-    return addr[device];
-}
-
 int cp_averages_noalloc(cp_handle* h, double out[22]) {
     if (!h || !out) return CP_E_ARG;
     if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_averages_noalloc: no mesh bound (JxW needed)");
@@ -1343,9 +1392,14 @@ int cp_averages_noalloc(cp_handle* h, double out[22]) {
     int64_t nblocks = 0;
     for (const auto& g : h->groups) nblocks += blocks_for(g.count, AVG_BLOCK);
     if (nblocks > NOALLOC_AVG_BLOCKS) return fail(h, CP_E_ARG, "cp_averages_noalloc: scratch too small");
-    cudaError_t e;
-    double* scratch = noalloc_avg_scratch(h->device, &e);
-    if (!scratch) return cuda_fail(h, e, "cp_averages_noalloc: cudaGetSymbolAddress");
+    // the array's device address (its host-side name is only a stand-in),
+    // looked up on the handle's first call with the handle's device current
+    if (!h->noalloc_scratch) {
+        void* p = nullptr;
+        CK(h, cudaGetSymbolAddress(&p, g_noalloc_avg_scratch));
+        h->noalloc_scratch = static_cast<double*>(p);
+    }
+    double* scratch = h->noalloc_scratch;
     double* partial = scratch;
     double* final_row = scratch + NOALLOC_AVG_BLOCKS * AVG_N;
     // every partial row read below is written earlier in this call, so the
@@ -1947,7 +2001,8 @@ int krylov_solve(cp_handle* h, const cp_solver_t& sv, const double* rhs, int hin
                      sv.precond_norm, sv.max_iterations, sv.rel_tolerance, bnorm, v(V_X), v(V_RES), v(V_RT),
                      v(V_Z), v(V_ZT), v(V_P), v(V_PT), v(V_Q), v(V_QT), v(V_S), v(V_T), s.d_fpartial,
                      s.d_ticket + 4, s.d_info,
-                     reinterpret_cast<int*>(s.d_ticket + 6), s.d_sc};
+                     reinterpret_cast<int*>(s.d_ticket + 6), s.d_sc,
+                     h->barrier_wait_ns ? h->barrier_wait_ns : PBICG_WAIT_NS, h->barrier_withhold};
         void* kargs[] = {&pa};
         CK(h, cudaLaunchCooperativeKernel((const void*)pbicg_kernel, dim3(p_grid), dim3(SOLVE_BLOCK), kargs, 0,
                                           h->stream));
@@ -2162,9 +2217,8 @@ int cp_solver_default(cp_solver_t* sv) {
 }
 
 
-int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
-                        const cp_solver_t* solver, cp_solve_info_t* info) {
-    if (!h) return CP_E_ARG;
+// the solver settings of a Newton iteration, checked (solver NULL: defaults)
+static int newton_settings(cp_handle* h, const cp_solver_t* solver, cp_solver_t* out) {
     auto& s = h->sys;
     if (!s.n_dofs) return fail(h, CP_E_STATE, "cp_newton_iteration: no dofs bound");
     cp_solver_t sv;
@@ -2188,17 +2242,51 @@ int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e
         (sv.kind != CP_SOLVER_BICG || sv.precond != CP_PRECOND_JACOBI || sv.precond_norm || sv.max_refinements < 0 ||
          !(sv.inner_tolerance >= 0.0 && sv.inner_tolerance < 1.0)))
         return fail(h, CP_E_UNSUPPORTED, "cp_newton_iteration: mixed precision runs Jacobi BiCG, true residual");
+    *out = sv;
+    return CP_OK;
+}
+
+static int newton_after_assembly(cp_handle* h, const cp_solver_t& sv, const double* h_du_constrained,
+                                 cp_solve_info_t* info);
+
+int cp_newton_iteration(cp_handle* h, const double* h_du_constrained, double F_e, double F_r,
+                        const cp_solver_t* solver, cp_solve_info_t* info) {
+    if (!h) return CP_E_ARG;
+    cp_solver_t sv;
+    if (int rc = newton_settings(h, solver, &sv)) return rc;
     if (int rc = check_device(h)) return rc;
     if (int rc = ensure_staging(h, false)) return rc;
     if (sv.precision == CP_PRECISION_MIXED) return mixed_newton_iteration(h, sv, h_du_constrained, F_e, F_r, info);
-    const int64_t n = s.n_dofs, nc = h->n_cells;
+    auto& s = h->sys;
+    const int64_t nc = h->n_cells;
+    // batched getElementalValues at the current u
+    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
+        s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
+    if (int rc = cp_assemble_device(h, s.d_Ul, F_e, F_r, s.d_Ke, s.d_Re, h->d_status)) return rc;
+    return newton_after_assembly(h, sv, h_du_constrained, info);
+}
+
+int cp_newton_solve(cp_handle* h, const double* h_du_constrained, const cp_solver_t* solver,
+                    cp_solve_info_t* info) {
+    if (!h) return CP_E_ARG;
+    cp_solver_t sv;
+    if (int rc = newton_settings(h, solver, &sv)) return rc;
+    if (sv.precision != CP_PRECISION_FP64)
+        return fail(h, CP_E_UNSUPPORTED, "cp_newton_solve: FP64 only (its Ke/Re come from cp_batch_assemble)");
+    if (int rc = check_device(h)) return rc;
+    if (int rc = ensure_staging(h, false)) return rc;
+    return newton_after_assembly(h, sv, h_du_constrained, info);
+}
+
+// K and R from the element matrices in sys.d_Ke / d_Re, condensation, the
+// Krylov solve, distribute and u += du
+static int newton_after_assembly(cp_handle* h, const cp_solver_t& sv, const double* h_du_constrained,
+                                 cp_solve_info_t* info) {
+    auto& s = h->sys;
+    const int64_t n = s.n_dofs;
     double* V = s.d_vec;
     auto v = [&](int k) { return V + (int64_t)k * n; };
     const unsigned nb = blocks_for(n, SOLVE_BLOCK);
-    // batched getElementalValues at the current u
-    gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(v(V_U), s.d_cell_dofs,
-                                                                                         24 * nc, s.d_Ul);
-    if (int rc = cp_assemble_device(h, s.d_Ul, F_e, F_r, s.d_Ke, s.d_Re, h->d_status)) return rc;
     // K and R (distribute_local_to_global), in cell order per entry
     scatter_sum_kernel<<<blocks_for(s.nnz, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(s.d_Ke, s.d_kptr, s.d_kidx,
                                                                                      s.nnz, s.d_vals);
@@ -2383,11 +2471,181 @@ int cp_autotune(cp_handle* h, const double* d_in, int32_t path, int32_t reps, do
     return rc == CP_OK ? ng : rc;
 }
 
+int cp_debug_barrier_test(cp_handle* h, int32_t withhold_block, double wait_seconds) {
+    if (!h || !(wait_seconds >= 0.0 && wait_seconds <= 60.0) || withhold_block < -1) return CP_E_ARG;
+    h->barrier_withhold = withhold_block;
+    h->barrier_wait_ns = (unsigned long long)(wait_seconds * 1e9);
+    return CP_OK;
+}
+
 int cp_graph_stats(cp_handle* h, int64_t* captures, int64_t* launches) {
     if (!h) return CP_E_ARG;
     if (captures) *captures = h->graph_captures;
     if (launches) *launches = h->graph_launches;
     return CP_OK;
+}
+
+// ---- continuous batching across handles ------------------------------------
+
+int cp_batch_create(int32_t device, cp_batch** out) {
+    if (!out) return CP_E_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return CP_E_CUDA;
+    cp_batch* b = new cp_batch();
+    b->device = device;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming) != cudaSuccess) {
+        cp_batch_destroy(b);
+        return CP_E_CUDA;
+    }
+    *out = b;
+    return CP_OK;
+}
+
+void cp_batch_destroy(cp_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto e : b->ev_in) cudaEventDestroy(e);
+    if (b->ev_done) cudaEventDestroy(b->ev_done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char* cp_batch_last_error(const cp_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int64_t cp_batch_launches(const cp_batch* b) { return b ? b->launches : 0; }
+
+static int batch_fail(cp_batch* b, int code, const std::string& msg) {
+    b->err = msg;
+    return code;
+}
+
+#define BCK(b, call)                                                                                  \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return batch_fail(b, CP_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// The sorted update of every lattice group of hs[0..n) at the displacement
+// each handle holds (its device u, as cp_newton_iteration gathers it), as
+// shared launches on the batch's stream: one counting sort over all groups
+// (per group keys and buckets) and one update launch per lattice class.
+// flag 1: the assembly (JxW P, JxW dP/dF staged, then each handle's
+// contraction into its system's Ke/Re); flag 0: the post-pass (F and T kept
+// for cp_averages).  Ordered after the work queued on each handle's stream
+// and before the work queued there afterwards.
+static int batch_run(cp_batch* b, cp_handle* const* hs, int32_t n, const double* F_e, const double* F_r, int flag) {
+    if (!b) return CP_E_ARG;
+    if (!hs || n < 1 || !F_e || !F_r) return batch_fail(b, CP_E_ARG, "cp_batch: bad arguments");
+    for (int i = 0; i < n; ++i) {
+        cp_handle* h = hs[i];
+        if (!h) return batch_fail(b, CP_E_ARG, "cp_batch: null handle");
+        if (h->device != b->device) return batch_fail(b, CP_E_ARG, "cp_batch: handle on another device");
+        if (!h->sys.n_dofs) return batch_fail(b, CP_E_STATE, "cp_batch: a handle has no dofs bound");
+        if (h->opts.plain_kernel) return batch_fail(b, CP_E_UNSUPPORTED, "cp_batch: needs the sorted update");
+        for (int j = 0; j < i; ++j)
+            if (hs[j] == h) return batch_fail(b, CP_E_ARG, "cp_batch: a handle is listed twice");
+    }
+    BCK(b, cudaSetDevice(b->device));
+    for (int i = 0; i < n; ++i) {
+        cp_handle* h = hs[i];
+        if (ensure_staging(h, false)) return batch_fail(b, CP_E_NOMEM, "cp_batch: " + h->err);
+        if (flag == 1 && !h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
+            return batch_fail(b, CP_E_NOMEM, "cp_batch: staging allocation failed");
+    }
+    while ((int)b->ev_in.size() < n) {
+        cudaEvent_t e;
+        BCK(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->ev_in.push_back(e);
+    }
+    for (int i = 0; i < n; ++i) {
+        BCK(b, cudaEventRecord(b->ev_in[i], hs[i]->stream));
+        BCK(b, cudaStreamWaitEvent(b->stream, b->ev_in[i], 0));
+    }
+    std::vector<BatchDesc> all;
+    for (int i = 0; i < n; ++i) {
+        cp_handle* h = hs[i];
+        auto& y = h->sys;
+        const int64_t nc = h->n_cells;
+        gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, b->stream>>>(
+            y.d_vec + V_U * y.n_dofs, y.d_cell_dofs, 24 * nc, y.d_Ul);
+        const FromMesh fm{y.d_Ul, h->d_gradN, h->d_JxW, h->uniform};
+        for (const auto& g : h->groups) {
+            BatchDesc d{};
+            d.L = h->d_lat[g.lattice];
+            d.o = h->dopts;
+            d.g = g.dev;
+            d.fm = fm;
+            d.key = g.d_key;
+            d.hist = g.d_hist;
+            d.perm = g.d_perm;
+            d.m = g.count;
+            d.F_e = F_e[i];
+            d.F_r = F_r[i];
+            d.stage = flag == 1 ? h->d_stage : nullptr;
+            d.status = h->d_status;
+            d.stats = h->d_stats;
+            d.keepF = flag == 0 ? h->d_keepF : nullptr;
+            d.keepT = flag == 0 ? h->d_keepT : nullptr;
+            d.lattice_id = g.lattice;
+            all.push_back(d);
+        }
+    }
+    // classes: the PMAX of each group's lattice, taken from its handle
+    std::vector<int> cls;
+    for (int i = 0; i < n; ++i)
+        for (const auto& g : hs[i]->groups) cls.push_back(g.nt_class == 16 ? 16 : (g.nt_class == 32 ? 32 : 48));
+    for (size_t c0 = 0; c0 < all.size(); c0 += CP_BATCH_MAX) {
+        const int cnt = (int)std::min<size_t>(CP_BATCH_MAX, all.size() - c0);
+        BatchArgs a;
+        a.n = cnt;
+        a.flag = flag;
+        int64_t b128 = 0, b256 = 0;
+        for (int k = 0; k < cnt; ++k) {
+            a.d[k] = all[c0 + k];
+            b128 += (a.d[k].m + QP_BLOCK - 1) / QP_BLOCK;
+            b256 += (a.d[k].m + 255) / 256;
+        }
+        batch_hist_zero_kernel<<<cnt, 2 * SORT_BUCKETS, 0, b->stream>>>(a);
+        if (b128) classify_batch_kernel<<<(unsigned)b128, QP_BLOCK, 0, b->stream>>>(a);
+        bucket_scan_batch_kernel<<<cnt, 32, 0, b->stream>>>(a);
+        if (b256) bucket_scatter_batch_kernel<<<(unsigned)b256, 256, 0, b->stream>>>(a);
+        BCK(b, cudaGetLastError());
+        for (int pm : {16, 32, 48}) {
+            BatchArgs u;
+            u.n = 0;
+            u.flag = flag;
+            for (int k = 0; k < cnt; ++k)
+                if (cls[c0 + k] == pm) u.d[u.n++] = all[c0 + k];
+            if (!u.n) continue;
+            cudaError_t e = pm == 16 ? launch_update2_batch<16>(b->stream, u)
+                                     : (pm == 32 ? launch_update2_batch<32>(b->stream, u)
+                                                 : launch_update2_batch<48>(b->stream, u));
+            if (e != cudaSuccess) return batch_fail(b, CP_E_CUDA, std::string("batched update: ") + cudaGetErrorString(e));
+            ++b->launches;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        cp_handle* h = hs[i];
+        if (flag == 1)
+            contract_kernel<<<blocks_for(h->n_cells, CONTRACT_CELLS), CONTRACT_CELLS * 8, 0, b->stream>>>(
+                h->d_stage, h->d_gradN, h->uniform, 0, h->n_cells, h->sys.d_Ke, h->sys.d_Re);
+        else
+            h->have_post = true;
+    }
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaEventRecord(b->ev_done, b->stream));
+    for (int i = 0; i < n; ++i) BCK(b, cudaStreamWaitEvent(hs[i]->stream, b->ev_done, 0));
+    return CP_OK;
+}
+
+int cp_batch_assemble(cp_batch* b, cp_handle* const* hs, int32_t n, const double* F_e, const double* F_r) {
+    return batch_run(b, hs, n, F_e, F_r, 1);
+}
+
+int cp_batch_post(cp_batch* b, cp_handle* const* hs, int32_t n, const double* F_e, const double* F_r) {
+    return batch_run(b, hs, n, F_e, F_r, 0);
 }
 
 }  // extern "C"

@@ -171,6 +171,49 @@ struct FromMesh {
     __device__ __forceinline__ double weight(int64_t k) const { return uniform ? JxW[k & 7] : JxW[k]; }
 };
 
+// ---------------------------------------------------------------- batched launches
+// One lattice group of one handle in a launch shared by several handles
+// (continuous batching of served requests): its constants, history, F
+// source (the cell's nodal displacements), sort buffers and outputs.  The
+// groups of a launch are laid out block-aligned: group k owns
+// ceil(m_k / blockDim) consecutive blocks, so no block spans two groups.
+struct BatchDesc {
+    const LatDev* L;
+    Opts o;
+    GroupDev g;
+    FromMesh fm;
+    unsigned char* key;
+    int* hist;  // SORT_BUCKETS counts, then SORT_BUCKETS offsets
+    int* perm;
+    int64_t m;
+    double F_e, F_r;
+    double* stage;  // assembly: JxW P, JxW dP/dF (null in the post-pass)
+    int32_t *status, *stats;
+    double *keepF, *keepT;  // post-pass: F and T kept for the averages
+    int lattice_id;
+};
+constexpr int CP_BATCH_MAX = 48;  // groups per batched launch (the launch parameter holds them by value)
+struct BatchArgs {
+    int n;
+    int flag;
+    BatchDesc d[CP_BATCH_MAX];
+};
+
+// the group owning this block (blocks of B threads, block-aligned layout)
+// and the block's index within it; -1 past the last group
+__device__ __forceinline__ int batch_group_of_block(const BatchArgs& a, int B, int64_t& local_block) {
+    int64_t b = blockIdx.x;
+    for (int k = 0; k < a.n; ++k) {
+        const int64_t nb = (a.d[k].m + B - 1) / B;
+        if (b < nb) {
+            local_block = b;
+            return k;
+        }
+        b -= nb;
+    }
+    return -1;
+}
+
 constexpr int SORT_BUCKETS = 64;
 
 // sort key: bucket 63 - min(p0, 63), so ascending buckets = descending p0
@@ -286,6 +329,23 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     if (j < m)
         update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
                           lattice_id, sD2 + threadIdx.x, BLOCK);
+}
+
+// update2_kernel over the groups of several handles in one launch: thread j
+// of group k's blocks runs internal qp perm_k[j] of that group (its own
+// constants, history and displacement field).  Same per-qp arithmetic as the
+// per-handle launch, so the results do not depend on what else shares it.
+template <int PMAX, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) update2_batch_kernel(const __grid_constant__ BatchArgs a) {
+    __shared__ double sD2[21 * BLOCK];
+    int64_t lb = 0;
+    const int k = batch_group_of_block(a, BLOCK, lb);
+    if (k < 0) return;
+    const BatchDesc& d = a.d[k];
+    const int64_t j = lb * BLOCK + threadIdx.x;
+    if (j < d.m)
+        update2_one<PMAX>(*d.L, d.o, d.g, d.fm, d.perm[j], a.flag, d.F_e, d.F_r, nullptr, nullptr, nullptr, d.stage,
+                          d.status, d.stats, d.keepF, d.keepT, d.lattice_id, sD2 + threadIdx.x, BLOCK);
 }
 
 #ifndef CP_TEMPLATES_ONLY

@@ -15,6 +15,7 @@ namespace cp {
 
 struct FromArray;
 struct FromMesh;
+struct BatchArgs;
 
 // Arguments of one sorted-update launch over m qps of a lattice group
 // (thread j runs internal qp perm[j]); see update2_kernel.
@@ -68,6 +69,12 @@ cudaError_t launch_assemble_plain(cudaStream_t s, const LatDev* L, const Opts& o
                                   const double* U, const double* gradN, const double* JxW, int uniform, double F_e,
                                   double F_r, double* Ke, double* Re, int32_t* status, int32_t* stats,
                                   int lattice_id);
+
+// The batched sorted update (update2_batch_kernel) of one lattice class over
+// the groups of several handles, in the class's default launch shape;
+// cp_batch_tu.cu, one translation unit per class.
+template <int PMAX>
+cudaError_t launch_update2_batch(cudaStream_t s, const BatchArgs& a, int64_t total_blocks_unused = 0);
 
 // Split-BF16 tensor-core contraction of the staged JxW dP/dF of cells
 // [cell_begin, cell_end) into FP32 Ke and, from the staged JxW P, FP64 Re

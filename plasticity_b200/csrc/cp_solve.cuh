@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK, SPMV3_MIN_BLOCKS) fbicg_spmv3_ker
 // PBICG_WAIT_NS of the global timer (or PBICG_SPIN_LIMIT polls) it raises err
 // and returns, and every block leaves at its next barrier once err is set, so
 // no launch can wait forever.
-constexpr long long PBICG_SPIN_LIMIT = 1ll << 24;
+constexpr long long PBICG_SPIN_LIMIT = 1ll << 30;  // a backstop only: the timer ends a wait first
 constexpr unsigned long long PBICG_WAIT_NS = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -526,16 +526,21 @@ struct PbicgArgs {
     int* info;         // [0] iterations, [1] converged, [2] breakdown
     int* err;          // barrier timeout
     double* sc;        // final scalars (SC_RR / SC_ZZ)
+    unsigned long long wait_ns;  // bound of one barrier wait
+    int withhold;      // diagnostics: this block never arrives at a barrier (-1: none)
 };
 
-__device__ __forceinline__ bool pbicg_barrier(unsigned* bar, int* err) {
+__device__ __forceinline__ bool pbicg_barrier(unsigned* bar, int* err, unsigned long long wait_ns = PBICG_WAIT_NS,
+                                              int withhold = -1) {
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned* gen = bar + 1;
         const unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        // (a withheld block skips its arrival and waits like the others, so
+        // every wait of the barrier runs out)
+        if ((int)blockIdx.x != withhold && atomicAdd(bar, 1u) == gridDim.x - 1) {
             bar[0] = 0u;
             __threadfence();
             atomicAdd(bar + 1, 1u);
@@ -543,7 +548,7 @@ __device__ __forceinline__ bool pbicg_barrier(unsigned* bar, int* err) {
             const unsigned long long t0 = global_ns();
             long long spins = 0;
             while (*gen == g) {
-                if (++spins > PBICG_SPIN_LIMIT || *(volatile int*)err || global_ns() - t0 > PBICG_WAIT_NS) {
+                if (++spins > PBICG_SPIN_LIMIT || *(volatile int*)err || global_ns() - t0 > wait_ns) {
                     atomicExch(err, 1);
                     break;
                 }
@@ -650,7 +655,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
         }
         pbicg_put(v, P0);
     }
-    if (!pbicg_barrier(a.bar, a.err)) return;
+    if (!pbicg_barrier(a.bar, a.err, a.wait_ns, a.withhold)) return;
     double rho = pbicg_allsum(P0), rho_old = 1.0;
     for (int k = 0; k < a.max_iter; ++k) {
         if (rho == 0.0 || !isfinite(rho)) {
@@ -740,7 +745,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
             }
             pbicg_put(v, P1);
         }
-        if (!pbicg_barrier(a.bar, a.err)) return;
+        if (!pbicg_barrier(a.bar, a.err, a.wait_ns, a.withhold)) return;
         const double den = pbicg_allsum(P1);
         if (den == 0.0 || !isfinite(den)) {
             if (lead) a.info[2] = 1;
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) pbicg_kernel(PbicgArgs a) {
             }
             pbicg_put2(vr, vz, P2, P0);
         }
-        if (!pbicg_barrier(a.bar, a.err)) return;
+        if (!pbicg_barrier(a.bar, a.err, a.wait_ns, a.withhold)) return;
         double rr;
         rho_old = rho;
         pbicg_allsum2(P2, P0, rr, rho);

@@ -335,17 +335,26 @@ class NewtonHarness:
         rhs[self.cdofs] = duc
         return spla.splu(K.tocsc()).solve(rhs)
 
+    def begin_increment(self):
+        """The increment's prescribed boundary values (moving boundaries)."""
+        if self.loading is not None:
+            self.cvals = self.loading.next_values(self.mesh, self.cdofs)
+
+    def constrained_increment(self, it):
+        """What Newton pass 'it' prescribes on the constrained dofs (the whole
+        increment on the first pass, nothing after)."""
+        return self.cvals if it == 0 else None
+
     def step(self):
         """One increment: max_newton assemble+solve passes, then the commit."""
         mesh = self.mesh
-        if self.loading is not None:
-            self.cvals = self.loading.next_values(mesh, self.cdofs)
+        self.begin_increment()
         if self.device_system:
             for it in range(self.max_newton):
-                self.solve_info.append(self.be.newton_iteration(self.cvals if it == 0 else None, self.F_e, self.F_r,
+                self.solve_info.append(self.be.newton_iteration(self.constrained_increment(it), self.F_e, self.F_r,
                                                                 self.solver))
             self.be.update_from_displacement(self.F_e, self.F_r)
-            self.u = self.be.get_displacement()
+            return self.finish_increment()
         else:
             for it in range(self.max_newton):
                 Ke, Re, st = self.be.assemble(self.u[mesh.cell_dofs], self.F_e, self.F_r)
@@ -355,6 +364,14 @@ class NewtonHarness:
                 self.u += self._solve(K, R, duc)
             F = mesh.deformation_gradients(self.u)
             self.be.update(F, 0, self.F_e, self.F_r)
+        return self.finish_increment()
+
+    def finish_increment(self):
+        """After the post-pass update: the volume averages, reorientation,
+        commit, the twin-rule scalars for the next increment and the
+        stress-strain row (updateAfterIncrement.cc)."""
+        if self.device_system:
+            self.u = self.be.get_displacement()
         avg = self.be.averages()
         self.be.reorient()
         self.be.commit()

@@ -14,9 +14,21 @@ cp_newton_iteration / cp_update_from_displacement) on a worker thread; the C
 calls release the interpreter lock, so requests in flight overlap on the
 device.  Latency is completion time minus arrival time.
 
+``BatchedRveServer`` is the continuous-batching form: the requests in
+flight advance in lockstep, one Newton pass (or the post-pass) per tick, and
+at every tick the calculatePlasticity work of all of them runs as shared
+launches (cp_batch_assemble / cp_batch_post: one update launch per lattice
+class over the qps of every request in flight); each request's global system
+is then solved on its own stream (cp_newton_solve, solves of different
+requests overlapping).  Requests join at the next tick after admission (their
+set-up runs meanwhile on a worker) and leave when their last increment is
+committed.
+
 This is host code over the C ABI (plasticity_b200.capi); the solve of a
 request does not depend on what else is in flight (every kernel of a handle
-runs on its own stream over its own buffers), which the GPU tests check.
+runs on its own stream over its own buffers, and a shared launch runs each
+qp with its own request's data and the same arithmetic), which the GPU tests
+check bit for bit.
 """
 from __future__ import annotations
 
@@ -197,6 +209,155 @@ class RveServer:
                     time.sleep(timeout)
                 elif waiting:  # nothing runs and nothing fits: cannot happen (oversize is rejected)
                     raise RuntimeError("server stalled")
+        return [results[k] for k in sorted(results)]
+
+
+@dataclasses.dataclass
+class _Live:
+    """A request in flight on the batched server."""
+    req: RveRequest
+    be: object
+    h: object
+    b: int            # its device-memory estimate
+    start: float
+    inc: int = 0      # committed increments
+    it: int = 0       # Newton passes done in the current increment
+
+
+class BatchedRveServer(RveServer):
+    """Continuous batching: admission as in RveServer (device-memory budget,
+    at most ``max_slots`` in flight, oldest first); the requests in flight
+    step together, their qp updates sharing launches (cp_batch_*), their
+    solves running concurrently on their own streams."""
+
+    def __init__(self, materials, budget_bytes: int, max_slots: int = 8, options_fn=None, solver=None,
+                 device: int = 0, max_newton: int = 4, setup_fn=None, batch_fn=None):
+        """setup_fn(request) -> (handle, harness) and batch_fn() -> batch queue
+        replace the device objects (the defaults build a CpHandle with its
+        NewtonHarness and a CpBatch)."""
+        super().__init__(materials, budget_bytes, max_slots, options_fn, solver)
+        self.device = device
+        self.max_newton = max_newton
+        self.setup_fn = setup_fn
+        self.batch_fn = batch_fn
+        self.ticks = 0
+        self.batched_launches = 0
+
+    def _prepare(self, req: RveRequest, t0: float, b: int) -> _Live:
+        if self.setup_fn is not None:
+            be, h = self.setup_fn(req)
+            return _Live(req, be, h, b, time.perf_counter() - t0)
+        from .capi import CpHandle, default_options, default_solver
+        mesh = H.StructuredMesh((req.edge, req.edge, req.edge))
+        lid, rod = req.microstructure(mesh)
+        be = CpHandle(self.materials, self.options_fn() if self.options_fn else default_options(device=self.device))
+        try:
+            be.bind_qps(lid, rod)
+            h = H.NewtonHarness(be, mesh, None, req.n_increments, self.max_newton, device_system=True,
+                                solver=self.solver or default_solver(), vel_grad=req.vel_grad, delT=req.delT)
+        except Exception:
+            be.close()
+            raise
+        return _Live(req, be, h, b, time.perf_counter() - t0)
+
+    def _solve_pass(self, lv: _Live):
+        lv.h.solve_info.append(lv.be.newton_solve(lv.h.constrained_increment(lv.it), lv.h.solver))
+
+    def run(self, requests):
+        if self.batch_fn is not None:
+            batch = self.batch_fn()
+        else:
+            from .capi import CpBatch
+            batch = CpBatch(self.device)
+        pending = deque(sorted(requests, key=lambda r: (r.arrival, r.rid)))
+        waiting: deque = deque()
+        setting_up = {}
+        live: list[_Live] = []
+        results = {}
+        used = 0
+        t0 = time.perf_counter()
+
+        def finish(lv, error=None):
+            nonlocal used
+            end = time.perf_counter() - t0
+            rows = np.array(lv.h.rows) if error is None else None
+            conv = error is None and all(i["converged"] for i in lv.h.solve_info)
+            results[lv.req.rid] = RveResult(lv.req.rid, rows, lv.req.arrival, lv.start, end, conv, error)
+            used -= lv.b
+            lv.be.close()
+
+        try:
+            with ThreadPoolExecutor(max_workers=2) as setup_pool, \
+                    ThreadPoolExecutor(max_workers=self.max_slots) as solve_pool:
+                while pending or waiting or setting_up or live:
+                    now = time.perf_counter() - t0
+                    while pending and pending[0].arrival <= now:
+                        waiting.append(pending.popleft())
+                    for req in list(waiting):
+                        b = self.bytes_of(req)
+                        if b > self.budget:
+                            waiting.remove(req)
+                            results[req.rid] = RveResult(req.rid, None, req.arrival, now, now, False,
+                                                         f"needs {b} bytes, budget {self.budget}")
+                            continue
+                        if len(live) + len(setting_up) < self.max_slots and used + b <= self.budget:
+                            waiting.remove(req)
+                            used += b
+                            setting_up[setup_pool.submit(self._prepare, req, t0, b)] = (req, b)
+                    # requests whose set-up finished join the next tick
+                    block = not live and setting_up
+                    for fut in list(setting_up):
+                        if block or fut.done():
+                            req, b = setting_up.pop(fut)
+                            try:
+                                live.append(fut.result())
+                            except Exception as e:
+                                used -= b
+                                t = time.perf_counter() - t0
+                                results[req.rid] = RveResult(req.rid, None, req.arrival, t, t, False, repr(e))
+                            block = False
+                    self.max_in_flight = max(self.max_in_flight, len(live))
+                    self.max_bytes_in_flight = max(self.max_bytes_in_flight, used)
+                    if not live:
+                        if not setting_up and pending:
+                            time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
+                        continue
+                    # one tick: a Newton pass of every request still in its Newton passes ...
+                    self.ticks += 1
+                    for lv in live:
+                        if lv.it == 0:
+                            lv.h.begin_increment()
+                    newton = [lv for lv in live if lv.it < self.max_newton]
+                    failed = []
+                    if newton:
+                        batch.assemble([lv.be for lv in newton], [lv.h.F_e for lv in newton],
+                                       [lv.h.F_r for lv in newton])
+                        futs = {solve_pool.submit(self._solve_pass, lv): lv for lv in newton}
+                        for fut, lv in futs.items():
+                            try:
+                                fut.result()
+                                lv.it += 1
+                            except Exception as e:
+                                failed.append((lv, repr(e)))
+                    for lv, err in failed:
+                        live.remove(lv)
+                        finish(lv, err)
+                    # ... then the post-pass and commit of those that finished them
+                    post = [lv for lv in live if lv.it == self.max_newton]
+                    if post:
+                        batch.post([lv.be for lv in post], [lv.h.F_e for lv in post], [lv.h.F_r for lv in post])
+                        for lv in post:
+                            lv.h.finish_increment()
+                            lv.inc += 1
+                            lv.it = 0
+                            if lv.inc == lv.req.n_increments:
+                                live.remove(lv)
+                                finish(lv)
+            self.batched_launches = batch.launches()
+        finally:
+            for lv in live:
+                lv.be.close()
+            batch.close()
         return [results[k] for k in sorted(results)]
 
 

@@ -1,8 +1,8 @@
 """Generate the known-answer fixtures tests/golden/kat_*.npz from the
 reference's own input decks and golden stress-strain curves.
 
-Run in a container where the reference checkout exists:
-    python tests/golden/make_fixtures.py /root/reference [case ...]
+Run where a reference checkout exists (its path is a required argument):
+    python tests/golden/make_fixtures.py <reference checkout> [case ...]
 
 For each case it stores what plasticity_b200.decks.load_deck reads from the
 deck (derived as the reference derives it):
@@ -58,4 +58,6 @@ def main(ref_root, only=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:])
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_fixtures.py <reference checkout> [case ...]")
+    main(sys.argv[1], sys.argv[2:])

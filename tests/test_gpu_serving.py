@@ -25,3 +25,22 @@ def test_results_identical_alone_and_in_the_mix(cuda_lib):
         assert a.rows.shape == (reqs[a.rid].n_increments, 15)
         assert np.array_equal(a.rows, b.rows)
     assert any(np.abs(r.rows[-1, 14]) > 0 for r in mixed)  # plastic slip in the mix
+
+
+def test_batched_serving_same_bits_as_one_at_a_time(cuda_lib):
+    """Continuous batching (BatchedRveServer: the qp updates of every request
+    in flight share launches) against the same requests solved one at a time
+    without batching: the same stress-strain rows, bit for bit."""
+    mats = [M.fcc_cu(), M.bcc_48(), M.hcp_mg()]
+    reqs = S.request_stream(6, rate=0.0, seed=11, edges=(4, 5, 6), grains=(4, 12), increments=(3, 5),
+                            norm=2e-3)
+    assert len({r.lattice for r in reqs}) > 1 and len({r.edge for r in reqs}) > 1
+    alone = S.RveServer(mats, budget_bytes=1 << 36, max_slots=1).run(reqs)
+    srv = S.BatchedRveServer(mats, budget_bytes=1 << 36, max_slots=6)
+    batched = srv.run(reqs)
+    assert srv.max_in_flight > 1 and srv.batched_launches >= srv.ticks
+    for a, b in zip(alone, batched):
+        assert a.error is None and b.error is None, (a.error, b.error)
+        assert a.converged and b.converged
+        assert np.array_equal(a.rows, b.rows), a.rid
+    assert any(np.abs(r.rows[-1, 14]) > 0 for r in batched)  # plastic slip in the mix

@@ -268,3 +268,37 @@ def test_device_newton_loading_modes(cuda_lib, case):
     assert err["stress"] < 2e-3 and err["strain"] < 2e-3, err
     hh.be.close()
     hd.be.close()
+
+
+def test_persistent_solve_barrier_wait_runs_out(cuda_lib):
+    """The cooperative Jacobi BiCG's grid barrier has a bounded wait.  With one
+    block made to withhold its arrival (a diagnostic switch; no fault, no
+    endless loop), every wait runs out after the set 0.2 s, the Newton
+    iteration returns CP_E_CUDA naming the barrier, the context stays usable,
+    and the same handle (switch off) and a fresh one then solve normally."""
+    import time
+    from plasticity_b200.capi import CP_E_CUDA
+    mesh = H.StructuredMesh((8, 8, 8))
+    rod = np.repeat(M.random_rodrigues(np.random.default_rng(0), mesh.n_cells), 8, axis=0)
+    bc = np.array([[1, 1, 0.0], [1, 2, 0.0], [1, 3, 0.0], [2, 1, 0.02]])
+
+    def handle():
+        be = CpHandle([M.fcc_cu()], default_options())
+        be.bind_qps(np.zeros(mesh.n_cells * 8, np.int32), rod)
+        h = H.NewtonHarness(be, mesh, bc, 20, 4, device_system=True)
+        return be, h
+
+    be, h = handle()
+    assert be.lib.cp_debug_barrier_test(be.h, 0, 0.2) == 0
+    t0 = time.perf_counter()
+    with pytest.raises(CpError, match="grid barrier"):
+        be.newton_iteration(h.cvals, 0.0, 0.0, default_solver(kernel_mode=2))
+    assert time.perf_counter() - t0 < 10.0
+    assert be.lib.cp_debug_barrier_test(be.h, -1, 0.0) == 0
+    info = be.newton_iteration(h.cvals, 0.0, 0.0, default_solver(kernel_mode=2))
+    assert info["converged"]
+    be.close()
+    be2, h2 = handle()
+    info2 = be2.newton_iteration(h2.cvals, 0.0, 0.0, default_solver(kernel_mode=2))
+    assert info2["converged"] and info2["iterations"] == info["iterations"]
+    be2.close()

@@ -99,3 +99,109 @@ def test_failed_solve_is_reported_not_raised():
     res = S.RveServer(mats, budget_bytes=1 << 40, max_slots=2, solve_fn=solve).run(reqs)
     assert res[1].rows is None and "broke down" in res[1].error
     assert res[0].rows is not None and res[2].rows is not None
+
+
+class _FakeHarness:
+    """Stands in for NewtonHarness in the batched server: records its phases."""
+
+    def __init__(self, req, log):
+        self.req, self.log = req, log
+        self.rows, self.solve_info, self.solver = [], [], None
+        self.F_e = self.F_r = 0.0
+
+    def begin_increment(self):
+        self.log.append(("begin", self.req.rid, len(self.rows)))
+
+    def constrained_increment(self, it):
+        return np.ones(3) if it == 0 else None
+
+    def finish_increment(self):
+        self.log.append(("finish", self.req.rid, len(self.rows)))
+        self.rows.append([float(self.req.rid)] * 15)
+        self.F_e = self.F_r = float(len(self.rows))
+
+
+class _FakeHandle:
+    def __init__(self, req, log, fail_at=None):
+        self.req, self.log, self.fail_at, self.solves, self.closed = req, log, fail_at, 0, False
+
+    def newton_solve(self, duc, solver):
+        self.solves += 1
+        if self.fail_at is not None and self.solves == self.fail_at:
+            raise RuntimeError("solver failed")
+        self.log.append(("solve", self.req.rid, duc is not None))
+        return {"converged": True, "iterations": 1}
+
+    def close(self):
+        self.closed = True
+
+
+class _FakeBatch:
+    def __init__(self, log):
+        self.log, self.calls, self.sizes = log, [], []
+
+    def assemble(self, handles, F_e, F_r):
+        assert len(handles) == len(F_e) == len(F_r)
+        self.calls.append("assemble")
+        self.sizes.append(len(handles))
+        self.log.append(("assemble", tuple(h.req.rid for h in handles)))
+
+    def post(self, handles, F_e, F_r):
+        self.calls.append("post")
+        self.log.append(("post", tuple(h.req.rid for h in handles)))
+
+    def launches(self):
+        return len(self.calls)
+
+    def close(self):
+        pass
+
+
+def _batched(reqs, max_slots=8, budget=1 << 40, fail=None):
+    log, handles = [], {}
+
+    def setup(req):
+        be = _FakeHandle(req, log, fail_at=fail.get(req.rid) if fail else None)
+        handles[req.rid] = be
+        return be, _FakeHarness(req, log)
+
+    fb = _FakeBatch(log)
+    srv = S.BatchedRveServer(_mats(), budget, max_slots, setup_fn=setup, batch_fn=lambda: fb)
+    return srv, srv.run(reqs), log, fb, handles
+
+
+def test_batched_server_steps_requests_together():
+    """Every tick is one shared assembly over all requests in their Newton
+    passes, a solve per request (the increment prescribed on the first pass
+    only), then one shared post-pass for those that finished their passes;
+    each request runs its own increments, in order, and its handle is
+    released when it completes."""
+    reqs = S.request_stream(6, rate=0.0, seed=3, increments=(2, 5), edges=(8,))
+    srv, res, log, fb, handles = _batched(reqs, max_slots=4)
+    assert [r.rid for r in res] == list(range(6))
+    for r in res:
+        assert r.error is None and r.converged and r.rows.shape == (reqs[r.rid].n_increments, 15)
+    assert max(fb.sizes) == 4 and srv.max_in_flight == 4  # four in flight share each launch
+    for rid, be in handles.items():
+        assert be.closed and be.solves == 4 * reqs[rid].n_increments
+        solves = [e[2] for e in log if e[0] == "solve" and e[1] == rid]
+        assert solves == [True, False, False, False] * reqs[rid].n_increments
+        inc = [e[2] for e in log if e[0] == "finish" and e[1] == rid]
+        assert inc == list(range(reqs[rid].n_increments))
+    # posts follow every fourth assembly of a request
+    for rid in handles:
+        seq = [e[0] for e in log if (e[0] in ("assemble", "post") and rid in e[1])]
+        assert seq == ["assemble"] * 4 + ["post"] + (["assemble"] * 4 + ["post"]) * (reqs[rid].n_increments - 1)
+
+
+def test_batched_server_admission_and_failures():
+    reqs = S.request_stream(5, rate=0.0, seed=4, increments=(2, 3), edges=(8, 12))
+    big = max(reqs, key=lambda r: r.edge)
+    budget = S.device_bytes(big, 13) * 2 + 1
+    srv, res, log, fb, handles = _batched(reqs, max_slots=8, budget=budget, fail={2: 3})
+    assert srv.max_bytes_in_flight <= budget
+    assert res[2].error is not None and res[2].rows is None and handles[2].closed
+    assert all(r.error is None for r in res if r.rid != 2)
+    # an oversize request is rejected at once
+    srv2, res2, _, _, _ = _batched(reqs, budget=S.device_bytes(min(reqs, key=lambda r: r.edge), 13) - 1)
+    assert all(r.error and "budget" in r.error for r in res2)
