@@ -447,6 +447,8 @@ def ours(args):
     rve_large = rve_large_leg(args, local, args.rve_large_increments) if (world == 1 and not args.no_rve_large) \
         else None
     dual = rve_dualphase_leg(args, local, args.rve_increments) if (world == 1 and not args.no_dualphase) else None
+    serve = serve_leg(args, local, args.serve_requests, tuple(float(x) for x in args.serve_rates.split(","))) \
+        if (world == 1 and not args.no_serve) else None
 
     line = {
         "metric": METRIC, "value": value, "unit": "qp-updates/s", "n_gpus": world, "steps": args.steps,
@@ -483,6 +485,7 @@ def ours(args):
         "rve": rve,
         "rve_large": rve_large,
         "rve_dualphase": dual,
+        "serve": serve,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -546,7 +549,7 @@ def assembly_leg(args, device):
     import torch
     from plasticity_b200 import harness as Hm
     from plasticity_b200.capi import CpHandle, default_options
-    n = ASM_N
+    n = args.asm_n
     nc = n ** 3
     rng = np.random.default_rng(SEED_LOAD + 7)
     lid = lattice_ids(nc)
@@ -886,38 +889,58 @@ def rve_dualphase_leg(args, device, increments=40):
     return out
 
 
-def serve_leg(args, device, n_requests=24, rates=(4.0, 16.0, 64.0), slots=8):
-    """The served RVE stream, sampled: n_requests independent RVE solves per
-    arrival rate (Poisson), edge 8/12/16 elements, FCC/BCC/HCP (the batched
-    workload's lattices), 8-64 Voronoi grains, 10-20 increments of a random
+def serve_leg(args, device, n_requests=16, rates=(4.0, 64.0), slots=8, edges=(8, 12, 16, 24, 32),
+              increments=(10, 50)):
+    """The served RVE stream: n_requests independent RVE solves per arrival
+    rate (Poisson), each a Q1 cube of edge^3 elements (edge drawn from
+    {8, 12, 16, 24, 32}), a lattice drawn from FCC/BCC/HCP (the batched
+    workload's), 8-64 Voronoi grains and 10-50 increments of a random
     traceless velocity gradient of norm 1e-3/s (dt = 1 s); admitted by a
     device-memory budget (80 % of the free memory) with up to ``slots`` in
-    flight.  Against the same requests served one at a time.  Reports
-    solves/s and p50/p95/p99 latency (completion minus arrival)."""
+    flight.  Three servers: the same requests one at a time with the plain
+    FP64 kernel (the baseline), concurrent requests each on its own handle
+    and stream, and continuous batching (the qp updates of all requests in
+    flight in shared launches).  Reports solves/s and p50/p95/p99 latency
+    (completion minus arrival) and checks that every batched result equals
+    its one-at-a-time result bit for bit."""
     import torch
     from plasticity_b200 import serving as S
+    from plasticity_b200.capi import default_options
     mats = materials()
     free, _ = torch.cuda.mem_get_info(device)
     budget = int(0.8 * free)
-    out = {"workload": f"{n_requests} RVE requests per rate: edge 8/12/16, FCC/BCC/HCP, 8-64 grains, "
-                       "10-20 increments of a random traceless velocity gradient (norm 1e-3/s)",
-           "slots": slots, "budget_gb": budget / 1e9}
+    out = {"workload": f"{n_requests} RVE requests per rate: edge {edges}, FCC/BCC/HCP, 8-64 grains, "
+                       f"{increments[0]}-{increments[1]} increments of a random traceless velocity gradient "
+                       "(norm 1e-3/s, dt 1 s)",
+           "slots": slots, "budget_gb": budget / 1e9, "rates_per_s": list(rates)}
     warm = S.request_stream(2, 0.0, 99, edges=(8,), increments=(2, 2))
-    S.RveServer(mats, budget, slots).run(warm)
-    base = S.request_stream(n_requests, 0.0, 6, edges=(8, 12, 16), increments=(10, 20))
+    S.RveServer(mats, budget, 1).run(warm)
+    S.BatchedRveServer(mats, budget, 2, device=device).run(warm)
+    base = S.request_stream(n_requests, 0.0, 6, edges=edges, increments=increments)
+    t0 = time.perf_counter()
+    plain = S.RveServer(mats, budget, 1, options_fn=lambda: default_options(device=device, plain_kernel=1)).run(base)
+    out["sequential_plain_fp64"] = S.summarize(plain, time.perf_counter() - t0)
     t0 = time.perf_counter()
     seq = S.RveServer(mats, budget, 1).run(base)
     out["sequential"] = S.summarize(seq, time.perf_counter() - t0)
     for rate in rates:
-        reqs = S.request_stream(n_requests, rate, 6, edges=(8, 12, 16), increments=(10, 20))
-        srv = S.RveServer(mats, budget, slots)
-        t0 = time.perf_counter()
-        res = srv.run(reqs)
-        summ = S.summarize(res, time.perf_counter() - t0)
-        summ["max_in_flight"] = srv.max_in_flight
-        summ["same_rows_as_sequential"] = bool(all(np.array_equal(a.rows, b.rows) for a, b in zip(seq, res)
-                                                   if a.rows is not None and b.rows is not None))
-        out[f"rate_{rate:g}"] = summ
+        reqs = S.request_stream(n_requests, rate, 6, edges=edges, increments=increments)
+        row = {}
+        for name, srv in (("concurrent", S.RveServer(mats, budget, slots)),
+                          ("batched", S.BatchedRveServer(mats, budget, slots, device=device))):
+            t0 = time.perf_counter()
+            res = srv.run(reqs)
+            summ = S.summarize(res, time.perf_counter() - t0)
+            summ["max_in_flight"] = srv.max_in_flight
+            summ["same_rows_as_sequential"] = bool(all(np.array_equal(a.rows, b.rows) for a, b in zip(seq, res)
+                                                       if a.rows is not None and b.rows is not None))
+            if name == "batched":
+                summ["ticks"] = srv.ticks
+                summ["shared_update_launches"] = srv.batched_launches
+            summ["solves_per_s_vs_sequential_plain_fp64"] = (summ["solves_per_s"]
+                                                             / out["sequential_plain_fp64"]["solves_per_s"])
+            row[name] = summ
+        out[f"rate_{rate:g}"] = row
     return out
 
 
@@ -935,12 +958,17 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuning before the timing")
     ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
+    ap.add_argument("--asm-n", type=int, default=ASM_N, help="cells per edge of the element-assembly leg's cube")
+    ap.add_argument("--assembly-only", action="store_true", help="only run the element-assembly leg")
     ap.add_argument("--rve-large", action="store_true", help="only run the 48^3 RVE leg")
     ap.add_argument("--rve-large-increments", type=int, default=50,
                     help="increments the 48^3 RVE leg runs (of its 50)")
     ap.add_argument("--no-rve-large", action="store_true", help="skip the 48^3 RVE leg")
     ap.add_argument("--no-dualphase", action="store_true", help="skip the 32^3 dual-phase RVE leg")
     ap.add_argument("--serve", action="store_true", help="only time the served RVE stream")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests per arrival rate of the serve leg")
+    ap.add_argument("--serve-rates", default="4,64", help="arrival rates (per s) of the serve leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served RVE stream leg")
     ap.add_argument("--rve-only", action="store_true", help="only time the 8^3 RVE solve on the device")
     ap.add_argument("--rve-increments", type=int, default=40,
                     help="increments the dual-phase RVE leg times (of its 40)")
@@ -955,6 +983,9 @@ def main():
         print(json.dumps({"rve_large": rve_large_leg(args, int(os.environ.get("LOCAL_RANK", "0")),
                                                      args.rve_large_increments)}), flush=True)
         return 0
+    if args.assembly_only:
+        print(json.dumps({"assembly": assembly_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        return 0
     if args.rve_only:
         from plasticity_b200.capi import CpHandle, default_options
         from plasticity_b200 import materials as M
@@ -968,7 +999,8 @@ def main():
         be.close()
         return 0
     if args.serve:
-        print(json.dumps({"serve": serve_leg(args, int(os.environ.get("LOCAL_RANK", "0")))}), flush=True)
+        print(json.dumps({"serve": serve_leg(args, int(os.environ.get("LOCAL_RANK", "0")), args.serve_requests,
+                                             tuple(float(x) for x in args.serve_rates.split(",")))}), flush=True)
         return 0
     if args.rve_dualphase:
         print(json.dumps({"rve_dualphase": rve_dualphase_leg(args, int(os.environ.get("LOCAL_RANK", "0")),

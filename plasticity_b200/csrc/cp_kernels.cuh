@@ -350,8 +350,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) update2_batch_kernel(const __grid
 
 #ifndef CP_TEMPLATES_ONLY
 // Element contraction (getElementalValues.cc:144-162) from the staged JxW*P
-// and JxW*dP/dF of the cell's 8 qps: thread (cell, node a) writes rows
-// 3a..3a+2 of Ke and Re.  Cells [cell_begin, cell_end) in caller order;
+// and JxW*dP/dF of the cell's 8 qps: thread (cell, node a) forms rows
+// 3a..3a+2 of Ke and Re; the block's Ke leave through shared memory as one
+// coalesced run.  Cells [cell_begin, cell_end) in caller order;
 // CONTRACT_CELLS per block.
 constexpr int CONTRACT_CELLS = 8;
 __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const double* __restrict__ stage,
@@ -359,7 +360,9 @@ __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const doub
                                                                       int64_t cell_begin, int64_t cell_end,
                                                                       double* __restrict__ Ke,
                                                                       double* __restrict__ Re) {
-    __shared__ double sd[CONTRACT_CELLS][8 * 90];
+    // one padded row per cell: the 8 threads of a cell read their own row,
+    // and a row stride of 721 doubles puts the warp's 4 cells on different banks
+    __shared__ double sd[CONTRACT_CELLS][8 * 90 + 1];
     const int tid = threadIdx.x;
     const int lc = tid >> 3, a1 = tid & 7;
     const int64_t cell0 = cell_begin + (int64_t)blockIdx.x * CONTRACT_CELLS;
@@ -369,8 +372,8 @@ __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const doub
     for (int t = tid; t < ncb * 720; t += CONTRACT_CELLS * 8) sd[t / 720][t % 720] = src[t];
     __syncthreads();
     const int64_t cell = cell0 + lc;
-    if (cell >= cell_end) return;
-    const double* g0 = uniform ? gradN : gradN + cell * 192;
+    const bool live = cell < cell_end;
+    const double* g0 = uniform ? gradN : gradN + (live ? cell : cell0) * 192;
     double K[3][24];
     double Rl[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -398,13 +401,24 @@ __global__ void __launch_bounds__(CONTRACT_CELLS * 8) contract_kernel(const doub
             }
         }
     }
-    double* Kc = Ke + cell * 576 + (3 * a1) * 24;
+    // Ke through shared memory (the staged values are no longer needed), so
+    // that the block's cells, contiguous in Ke, are written coalesced
+    __syncthreads();
+    if (live) {
+        double* Ks = &sd[lc][(3 * a1) * 24];
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int c = 0; c < 24; ++c) Kc[r * 24 + c] = K[r][c];
+            for (int c = 0; c < 24; ++c) Ks[r * 24 + c] = K[r][c];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) Re[cell * 24 + 3 * a1 + r] = Rl[r];
+        for (int r = 0; r < 3; ++r) Re[cell * 24 + 3 * a1 + r] = Rl[r];
+    }
+    __syncthreads();
+    double2* dst = reinterpret_cast<double2*>(Ke + cell0 * 576);
+    for (int t = tid; t < ncb * 288; t += CONTRACT_CELLS * 8) {
+        const int cc = t / 288, e = t % 288;
+        dst[t] = make_double2(sd[cc][2 * e], sd[cc][2 * e + 1]);
+    }
 }
 
 #endif

@@ -63,6 +63,16 @@ static_assert(TC_OFF_A >= TC_IN_DOUBLES * 8, "input staging overlaps the operand
 static_assert(TC_CELLS * 9 <= TC_M, "a tile's rows exceed the MMA's M");
 static_assert(TC_SMEM <= 232448, "more shared memory than a CTA may have");
 
+// column t = 9 q + 3 k + l of A (t < 72) -> offset of JxW dP/dF[i][k][j][l]
+// of qp q in a cell's staged record, relative to that of [i][0][j][0] of qp 0
+// (records of 90 doubles: 9 of JxW P, then 81 of JxW dP/dF)
+__constant__ short c_tc_off[TC_KREAL] = {
+#define CP_TC_OFF(q) 90 * q, 90 * q + 1, 90 * q + 2, 90 * q + 9, 90 * q + 10, 90 * q + 11, 90 * q + 18, \
+                     90 * q + 19, 90 * q + 20
+    CP_TC_OFF(0), CP_TC_OFF(1), CP_TC_OFF(2), CP_TC_OFF(3), CP_TC_OFF(4), CP_TC_OFF(5), CP_TC_OFF(6), CP_TC_OFF(7)
+#undef CP_TC_OFF
+};
+
 // byte offset of element (r, k) of a K-major operand tile (r: M or N index)
 __device__ __forceinline__ int kmajor_off(int r, int k) {
     return (r >> 3) * TC_ROWBYTES + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
@@ -229,15 +239,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (*s_err) break;
         load_phase ^= 1u;
         if (tid == 0) load_pending = false;
-        // A[m = 9 c + 3 i + j][t = 9 q + 3 k + l] = JxW dP/dF[i][k][j][l] of qp q of cell c, split
-        for (int e = tid; e < nc * 648; e += TC_THREADS) {
-            const int c = e / 648, r = e % 648, q = r / 81, d = r % 81;
-            const int i = d / 27, k = (d / 9) % 3, j = (d / 3) % 3, l = d % 3;
-            unsigned short h[3];
-            split3(sIn[(c * 8 + q) * 90 + 9 + d], h);
-            const int off = kmajor_off(9 * c + 3 * i + j, 9 * q + 3 * k + l);
+        // A[m = 9 c + 3 i + j][t = 9 q + 3 k + l] = JxW dP/dF[i][k][j][l] of qp q
+        // of cell c, split.  Work item (row m, chunk kc) fills columns
+        // t = 8 kc .. 8 kc + 7 of the row: one 16-byte store per bf16 term;
+        // the 32 lanes of a warp take consecutive rows of one chunk, so the
+        // column offsets (c_tc_off) are the same in every lane
+        for (int e = tid; e < (TC_KREAL / 8) * TC_M; e += TC_THREADS) {
+            const int kc = e / TC_M, m = e % TC_M;
+            if (m >= 9 * nc) continue;
+            const int c = m / 9, r9 = m % 9;
+            const double* row = sIn + c * 720 + 9 + 27 * (r9 / 3) + 3 * (r9 % 3);
+            uint32_t w[3][4];
 #pragma unroll
-            for (int p = 0; p < 3; ++p) *reinterpret_cast<unsigned short*>(sA + p * TC_A_BYTES + off) = h[p];
+            for (int u = 0; u < 4; ++u) {
+                unsigned short h0[3], h1[3];
+                split3(row[c_tc_off[8 * kc + 2 * u]], h0);
+                split3(row[c_tc_off[8 * kc + 2 * u + 1]], h1);
+#pragma unroll
+                for (int p = 0; p < 3; ++p) w[p][u] = (uint32_t)h0[p] | ((uint32_t)h1[p] << 16);
+            }
+            const int off = kmajor_off(m, 8 * kc);
+#pragma unroll
+            for (int p = 0; p < 3; ++p)
+                *reinterpret_cast<uint4*>(sA + p * TC_A_BYTES + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
         }
         // Re in FP64 from JxW P, in contract_kernel's order of operations
         for (int e = tid; e < nc * 24; e += TC_THREADS) {
