@@ -523,11 +523,28 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
 
     ok = (sg[:, 7] <= 12) & (so_[:, 7] <= 12)  # well-posed active-set solves on both sides
     same = np.all(sg[:, :3] == so_[:, :3], axis=1)
+    # the oracle against itself compiled with fused multiply-adds (another
+    # valid rounding of the same arithmetic): where the active-set solves are
+    # ill conditioned, the reference's own result is set by rounding
+    prev = O.use_library(O.build_fma())
+    try:
+        for f in ("Fp", "Fe", "s", "W", "rot", "rotnew", "twinfrac", "slipfrac", "twin"):
+            for suf in ("_conv", "_iter"):
+                be.set_state(f + suf, h.get_state(f + suf)[:n_s])
+        be.update(Fh, 1)
+        sf = be.stats()
+    finally:
+        O.restore_library(prev)
+    okf = (sf[:, 7] <= 12) & (so_[:, 7] <= 12)
+    samef = np.all(sf[:, :3] == so_[:, :3], axis=1)
     parity = {"sample_qps": n_s, "well_posed_qps": int(ok.sum()),
               "max_rel_err_P": rel(Pg[ok], Po[ok]), "max_rel_err_dPdF": rel(Dg[ok], Do[ok]),
               "active_sets_identical": bool(same[ok].all()), "tolerance": 1e-10,
               "ill_conditioned_qps": int((~ok).sum()),
               "ill_conditioned_active_set_mismatches": int((~same[~ok]).sum()),
+              "oracle_fma_build_vs_oracle": {"ill_conditioned_qps": int((~okf).sum()),
+                                             "ill_conditioned_active_set_mismatches": int((~samef[~okf]).sum()),
+                                             "well_posed_active_sets_identical": bool(samef[okf].all())},
               "criterion": "identical active sets and <=1e-10 on qps whose active-set solves have condition <= 1e12"}
     cpu = {"value": n_s / dt, "unit": "qp-updates/s", "cores": threads, "kind": "port",
            "sample": f"first {n_s} qps of the workload (GPU's history, same F), one flag-1 update"}

@@ -45,23 +45,51 @@ def build(force: bool = False) -> str:
 _lib = None
 
 
+def build_fma() -> str:
+    """The oracle compiled with fused multiply-adds allowed (make fma)."""
+    path = os.path.join(_HERE, "_build", "libcp_oracle_fma.so")
+    if not os.path.exists(path):
+        subprocess.run(["make", "-C", _HERE, "fma"], check=True, capture_output=True)
+    return path
+
+
+def use_library(path: str | None):
+    """Route the module's calls to the oracle library at 'path' (None: the
+    default build); returns the previous library so a caller can restore it."""
+    global _lib
+    prev = _lib
+    _lib = None
+    if path is not None:
+        _lib = _load(path)
+    return prev
+
+
+def restore_library(prev):
+    global _lib
+    _lib = prev
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        L = C.CDLL(build())
-        M, O, S = C.POINTER(CpMaterial), C.POINTER(CpOptions), C.POINTER(OrState)
-        L.oracle_update.argtypes = [M, O, S, D, C.c_int32, C.c_double, C.c_double, D, D, D, I32, I32, C.c_int32]
-        L.oracle_assemble.argtypes = [M, O, S, C.c_int64, D, D, D, C.c_int32, C.c_double, C.c_double,
-                                      D, D, I32, I32, C.c_int32]
-        L.oracle_reorient.argtypes = [S, C.c_int32]
-        L.oracle_odfpoint.argtypes = [D, D]
-        L.oracle_elasticmoduli.argtypes = [D, D, D]
-        L.oracle_matrix_exponential.argtypes = [D, D]
-        L.oracle_pinv_svd.argtypes = [D, C.c_int, D]
-        L.oracle_invert.argtypes = [D, C.c_int, D]
-        L.oracle_eig_sym3.argtypes = [D, D, D]
-        _lib = L
+        _lib = _load(build())
     return _lib
+
+
+def _load(path) -> C.CDLL:
+    L = C.CDLL(path)
+    M, O, S = C.POINTER(CpMaterial), C.POINTER(CpOptions), C.POINTER(OrState)
+    L.oracle_update.argtypes = [M, O, S, D, C.c_int32, C.c_double, C.c_double, D, D, D, I32, I32, C.c_int32]
+    L.oracle_assemble.argtypes = [M, O, S, C.c_int64, D, D, D, C.c_int32, C.c_double, C.c_double,
+                                  D, D, I32, I32, C.c_int32]
+    L.oracle_reorient.argtypes = [S, C.c_int32]
+    L.oracle_odfpoint.argtypes = [D, D]
+    L.oracle_elasticmoduli.argtypes = [D, D, D]
+    L.oracle_matrix_exponential.argtypes = [D, D]
+    L.oracle_pinv_svd.argtypes = [D, C.c_int, D]
+    L.oracle_invert.argtypes = [D, C.c_int, D]
+    L.oracle_eig_sym3.argtypes = [D, D, D]
+    return L
 
 
 def _p(a):
