@@ -358,6 +358,9 @@ cudaError_t launch_ke_tc(cudaStream_t s, const double* stage, const double* grad
                          int64_t cell_end, float* Ke, double* Re, int* err, int num_sms) {
     const int64_t ntiles = (cell_end - cell_begin + TC_CELLS - 1) / TC_CELLS;
     if (ntiles <= 0) return cudaSuccess;
+    // the bulk copies start at stage + 720 * cell (5,760 B per cell): 16-byte
+    // alignment of every copy follows from the base's
+    if (reinterpret_cast<uintptr_t>(stage) & 15u) return cudaErrorInvalidValue;
     const unsigned grid = (unsigned)(ntiles < num_sms ? ntiles : num_sms);
     ke_tc_kernel<<<grid, TC_THREADS, TC_SMEM, s>>>(stage, gradN, cell_begin, cell_end, Ke, Re, err);
     return cudaGetLastError();

@@ -44,3 +44,39 @@ def test_batched_serving_same_bits_as_one_at_a_time(cuda_lib):
         assert a.converged and b.converged
         assert np.array_equal(a.rows, b.rows), a.rid
     assert any(np.abs(r.rows[-1, 14]) > 0 for r in batched)  # plastic slip in the mix
+
+
+def test_admission_estimate_bounds_actual_device_memory(cuda_lib):
+    """serving.device_bytes (the admission estimate) against the drop in the
+    device's free memory that a request's set-up and first increment cause,
+    after a warm-up request of the same lattice has loaded the kernels and
+    the local-memory reservation."""
+    import torch
+    from plasticity_b200.capi import CpHandle, default_options, default_solver
+    from plasticity_b200 import harness as H
+    mats = [M.fcc_cu(), M.bcc_48(), M.hcp_mg()]
+    srv = S.RveServer(mats, budget_bytes=1 << 36, max_slots=1)
+    warm = S.request_stream(1, rate=0.0, seed=3, edges=(4,), grains=(4, 5), increments=(2, 3))[0]
+    warm.lattice = 1
+    rows, conv = srv._device_solve(warm)
+    assert conv
+    for edge in (8, 12):
+        req = S.request_stream(1, rate=0.0, seed=edge, edges=(edge,), grains=(8, 9), increments=(2, 3))[0]
+        req.lattice = 1
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(0)
+        mesh = H.StructuredMesh((edge, edge, edge))
+        lid, rod = req.microstructure(mesh)
+        be = CpHandle(mats, default_options())
+        try:
+            be.bind_qps(lid, rod)
+            h = H.NewtonHarness(be, mesh, None, req.n_increments, 4, device_system=True,
+                                solver=default_solver(), vel_grad=req.vel_grad, delT=req.delT)
+            h.run(1)
+            torch.cuda.synchronize()
+            free1, _ = torch.cuda.mem_get_info(0)
+        finally:
+            be.close()
+        used = free0 - free1
+        est = srv.bytes_of(req)
+        assert 0 < used <= est, (edge, used, est)
