@@ -441,7 +441,7 @@ def ours(args):
     cpu = None
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, parity = cpu_leg(args, h, Fn, P, dPdF, lid, rod)
+        cpu, parity = cpu_leg(args, h, Fn, P, dPdF, lid, rod, local)
     asm = assembly_leg(args, local) if (world == 1 and not args.no_assembly) else None
     rve = rve_leg(args, local) if (world == 1 and not args.no_rve) else None
     rve_large = rve_large_leg(args, local, args.rve_large_increments) if (world == 1 and not args.no_rve_large) \
@@ -496,7 +496,7 @@ def ours(args):
     return 0
 
 
-def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
+def cpu_leg(args, h, Fn, P, dPdF, lid, rod, device=0):
     """Oracle on the first qps of this exact workload: the GPU's conv state of
     those qps and the same F; times one flag-1 update on all host cores and
     compares it with the GPU's P and dP/dF for those qps."""
@@ -537,6 +537,7 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
         O.restore_library(prev)
     okf = (sf[:, 7] <= 12) & (so_[:, 7] <= 12)
     samef = np.all(sf[:, :3] == so_[:, :3], axis=1)
+    ref_order = reference_order_parity(h, Fh, lid[:n_s], rod[:n_s], n_s, threads, device)
     parity = {"sample_qps": n_s, "well_posed_qps": int(ok.sum()),
               "max_rel_err_P": rel(Pg[ok], Po[ok]), "max_rel_err_dPdF": rel(Dg[ok], Do[ok]),
               "active_sets_identical": bool(same[ok].all()), "tolerance": 1e-10,
@@ -545,10 +546,56 @@ def cpu_leg(args, h, Fn, P, dPdF, lid, rod):
               "oracle_fma_build_vs_oracle": {"ill_conditioned_qps": int((~okf).sum()),
                                              "ill_conditioned_active_set_mismatches": int((~samef[~okf]).sum()),
                                              "well_posed_active_sets_identical": bool(samef[okf].all())},
+              "reference_order": ref_order,
               "criterion": "identical active sets and <=1e-10 on qps whose active-set solves have condition <= 1e12"}
     cpu = {"value": n_s / dt, "unit": "qp-updates/s", "cores": threads, "kind": "port",
            "sample": f"first {n_s} qps of the workload (GPU's history, same F), one flag-1 update"}
     return cpu, parity
+
+
+def reference_order_parity(h, Fh, lid, rod, n_s, threads, device=0):
+    """The library's reference-order update (cp_options_t.reference_order)
+    on the GPU against the oracle's parity build on the CPU, both from the
+    GPU's history of the sample's qps with the same F: qps whose outputs (P,
+    dP/dF, status, statistics, the whole _iter history) differ in any bit."""
+    from oracle import oracle as O
+    from plasticity_b200.capi import CpHandle, default_options
+    fields = ("Fp", "Fe", "s", "W", "rot", "rotnew", "twinfrac", "slipfrac", "twin")
+    out_fields = [f + "_iter" for f in fields]
+    g = CpHandle(materials(), default_options(device=device, reference_order=1))
+    g.bind_qps(lid, rod)
+    prev = O.use_library(O.build_parity())
+    try:
+        be = O.OracleBackend(materials(), default_options(), nthreads=threads)
+        be.bind_qps(lid, rod)
+        for f in fields:
+            for suf in ("_conv", "_iter"):
+                v = h.get_state(f + suf)[:n_s]
+                be.set_state(f + suf, v)
+                g.set_state(f + suf, v)
+        t0 = time.perf_counter()
+        Pg, _, Dg, sgs = g.update(Fh, 1)
+        t_gpu = time.perf_counter() - t0
+        Po, _, Do, sos = be.update(Fh, 1)
+        stg, sto = g.stats(), be.stats()
+
+        def same(a, b):
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(len(a), -1)
+            b = np.ascontiguousarray(b, dtype=np.float64).reshape(len(b), -1)
+            return ((a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))).all(axis=1)
+
+        ok = same(Pg, Po) & same(Dg, Do) & (sgs == sos) & (stg[:, :6] == sto[:, :6]).all(axis=1)
+        for f in out_fields:
+            ok &= same(g.get_state(f), be.get_state(f))
+    finally:
+        O.restore_library(prev)
+        g.close()
+    ill = sto[:, 7] > 12
+    return {"sample_qps": n_s, "ill_conditioned_qps": int(ill.sum()),
+            "mismatching_qps": int((~ok).sum()), "ill_conditioned_mismatching_qps": int((~ok & ill).sum()),
+            "gpu_seconds": t_gpu,
+            "criterion": "cp_options_t.reference_order on the GPU vs the oracle's parity build: every output "
+                         "bit (P, dP/dF, status, stats, _iter history) at every qp"}
 
 
 # --------------------------------------------------------------------- assembly

@@ -110,6 +110,13 @@ typedef struct cp_options_t {
                                            scratch (the plain FP64 drop-in, kept as a baseline);
                                            0 (default): qps sorted by potentially-active-set size each
                                            call, compact per-thread scratch */
+    int32_t reference_order;            /* 1: cp_update / cp_update_device / cp_update_from_displacement
+                                           evaluate calculatePlasticity in the reference's own operation
+                                           order (full consistency matrix, SVD pseudo-inverse, FullMatrix
+                                           inverses, no multiply-add contraction), reproducing a CPU
+                                           restatement bit for bit; slow (per-qp scratch of ~6 n^2
+                                           doubles, up to 2 GiB per handle).  The assembly, autotune,
+                                           mixed-precision and batch calls return CP_E_UNSUPPORTED. */
 } cp_options_t;
 
 typedef struct cp_handle cp_handle;

@@ -23,6 +23,73 @@ namespace {
 
 constexpr int NM = CP_MAX_SYSTEMS;
 
+/* ---- the parity build (-DCP_ORACLE_PARITY, libcp_oracle_parity.so) -------
+ * std::pow, std::tgamma and std::cos(std::atan(.)) are glibc's; a GPU has its
+ * own.  The parity build replaces them with functions made only of correctly
+ * rounded operations, so that a device evaluation of the same operations
+ * (cp_options_t.reference_order) reproduces this build bit for bit:
+ *   pow(x, y) = exp(y log x): log by 2 atanh((m-1)/(m+1)) on the mantissa
+ *   m in [sqrt(1/2), sqrt(2)) (12 series terms in s^2), exp by Cody-Waite
+ *   reduction with ln 2 split in two and 18 nested Taylor terms;
+ *   tgamma(k + 2) = (k+1)! as the product 2 * 3 * ... * (k+1);
+ *   cos(atan(r)) = 1 / sqrt(1 + r^2). */
+const double P_LN2_HI = 0.693147180369123816490;
+const double P_LN2_LO = 1.90821492927058770002e-10;
+const double P_INV_LN2 = 1.44269504088896338700;
+const double P_SQRT_HALF = 0.70710678118654752440;
+
+double parity_log(double x) {
+    int e = 0;
+    double m = std::frexp(x, &e);
+    if (m < P_SQRT_HALF) {
+        m = m * 2.0;
+        e = e - 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double z = s * s;
+    double p = 1.0 / 25.0;
+    for (int j = 11; j >= 0; --j) p = p * z + 1.0 / (double)(2 * j + 1);
+    const double lnm = (2.0 * s) * p;
+    const double de = (double)e;
+    return (de * P_LN2_HI + lnm) + de * P_LN2_LO;
+}
+double parity_exp(double t) {
+    if (t != t) return t;
+    if (t > 709.782712893384) return INFINITY;
+    if (t < -745.2) return 0.0;
+    const double kd = std::floor(t * P_INV_LN2 + 0.5);
+    const double r = (t - kd * P_LN2_HI) - kd * P_LN2_LO;
+    double p = 1.0;
+    for (int j = 18; j >= 1; --j) p = 1.0 + (r / (double)j) * p;
+    return std::ldexp(p, (int)kd);
+}
+double parity_pow(double x, double y) {
+    if (y == 0.0 || x == 1.0) return 1.0;
+    if (x != x || y != y) return x + y;
+    if (x == 0.0) return y > 0.0 ? 0.0 : INFINITY;
+    double ax = x, sign = 1.0;
+    if (x < 0.0) {
+        if (std::floor(y) != y) return (x - x) / (x - x);
+        ax = -x;
+        if (std::fmod(y, 2.0) != 0.0) sign = -1.0;
+    }
+    if (ax == INFINITY) return sign * (y > 0.0 ? INFINITY : 0.0);
+    return sign * parity_exp(y * parity_log(ax));
+}
+#ifdef CP_ORACLE_PARITY
+inline double o_pow(double x, double y) { return parity_pow(x, y); }
+inline double o_fact(int k) {  /* (k+1)! = tgamma(k + 2) */
+    double f = 1.0;
+    for (int j = 1; j <= k; ++j) f = f * (double)(j + 1);
+    return f;
+}
+inline double o_cos_atan(double r2) { return 1.0 / std::sqrt(1.0 + r2); }
+#else
+inline double o_pow(double x, double y) { return std::pow(x, y); }
+inline double o_fact(int k) { return std::tgamma(k + 2); }
+inline double o_cos_atan(double r2) { return std::cos(std::atan(std::sqrt(r2))); }
+#endif
+
 /* ---- 3x3 helpers with deal.II FullMatrix call semantics ------------------ */
 struct M3 {
     double a[3][3];
@@ -516,7 +583,7 @@ int inactive_slip_removal(int n, std::vector<int>& PA, const double* b,
 /* rod2quat / quatproduct / quat2rod, updateAfterIncrement.cc:781-821 */
 void rod2quat(double quat[4], const double rod[3]) {
     const double dotrod = rod[0] * rod[0] + rod[1] * rod[1] + rod[2] * rod[2];
-    const double cphiby2 = std::cos(std::atan(std::sqrt(dotrod)));
+    const double cphiby2 = o_cos_atan(dotrod);
     quat[0] = cphiby2;
     quat[1] = cphiby2 * rod[0];
     quat[2] = cphiby2 * rod[1];
@@ -552,7 +619,7 @@ M3 gateaux_series(const M3& S, const M3& dFp, int count3, bool alternating) {
             M3 t6 = mmult(t5, t2);
             add3(t4, 1.0, t6);
         }
-        const double coef = (alternating ? std::pow(-1.0, k) : 1.0) / std::tgamma(k + 2);
+        const double coef = (alternating ? ((k & 1) ? -1.0 : 1.0) : 1.0) / o_fact(k);
         t4 = scale3(coef, t4);
         add3(diff, 1.0, t4);
     }
@@ -682,9 +749,9 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
 
         /* :250-306 hardening moduli and the consistency matrix A */
         for (int i = 0; i < ns; ++i)
-            h_beta[i] = L.h0[i] * std::pow((1 - s_alpha_tau[i] / L.ss[i]), L.a[i]);
+            h_beta[i] = L.h0[i] * o_pow((1 - s_alpha_tau[i] / L.ss[i]), L.a[i]);
         for (int i = 0; i < nw; ++i)
-            h_beta[ns + i] = L.h0[ns + i] * std::pow((1 - s_alpha_tau[ns + i] / L.ss[ns + i]), L.a[ns + i]);
+            h_beta[ns + i] = L.h0[ns + i] * o_pow((1 - s_alpha_tau[ns + i] / L.ss[ns + i]), L.a[ns + i]);
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) {
                 h_ab[(size_t)i * NM + j] = L.q[(size_t)i * NM + j] * h_beta[j];
@@ -843,9 +910,9 @@ int calculate_plasticity(const Lattice& L, const cp_options_t& opt, const or_sta
             /* :548-579 hardening sensitivity; dels_delF = inv(I - term_ds) dels_delF_prev */
             double delh[NM];
             for (int i = 0; i < ns; ++i)
-                delh[i] = L.h0[i] * std::pow((1 - s_alpha_tau[i] / L.ss[i]), (L.a[i] - 1)) * (-1.0 / L.ss[i]);
+                delh[i] = L.h0[i] * o_pow((1 - s_alpha_tau[i] / L.ss[i]), (L.a[i] - 1)) * (-1.0 / L.ss[i]);
             for (int i = 0; i < nw; ++i)
-                delh[ns + i] = L.h0[ns + i] * std::pow((1 - s_alpha_tau[ns + i] / L.ss[ns + i]), (L.a[ns + i] - 1)) *
+                delh[ns + i] = L.h0[ns + i] * o_pow((1 - s_alpha_tau[ns + i] / L.ss[ns + i]), (L.a[ns + i] - 1)) *
                                (-1.0 / L.ss[ns + i]);
             {
                 std::vector<double> Im((size_t)n * n), Iinv((size_t)n * n);
@@ -1254,6 +1321,8 @@ int oracle_matrix_exponential(const double A[9], double out[9]) {
 int oracle_pinv_svd(const double* A, int n, double* Ainv) { return pinv_svd(A, n, Ainv, nullptr); }
 
 int oracle_invert(const double* A, int n, double* Ainv) { return invert_n(A, n, Ainv); }
+
+double oracle_parity_pow(double x, double y) { return parity_pow(x, y); }
 
 void oracle_eig_sym3(const double C[9], double evals[3], double evecs[9]) {
     M3 V;

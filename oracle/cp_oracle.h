@@ -67,6 +67,8 @@ int oracle_matrix_exponential(const double A[9], double out[9]);
 int oracle_pinv_svd(const double* A, int n, double* Ainv);
 int oracle_invert(const double* A, int n, double* Ainv);
 void oracle_eig_sym3(const double C[9], double evals[3], double evecs[9]);
+/* the parity build's pow (exported by every build, used by the parity build) */
+double oracle_parity_pow(double x, double y);
 
 #ifdef __cplusplus
 }

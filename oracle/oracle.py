@@ -36,8 +36,17 @@ class OrState(C.Structure):
     ] + [("twin_iter", I32)]
 
 
+def _stale(path) -> bool:
+    if not os.path.exists(path):
+        return True
+    t = os.path.getmtime(path)
+    srcs = [os.path.join(_HERE, f) for f in ("cp_oracle.cpp", "cp_oracle.h", "Makefile")]
+    srcs.append(os.path.join(os.path.dirname(_HERE), "include", "cp_gpu.h"))
+    return any(os.path.exists(f) and os.path.getmtime(f) > t for f in srcs)
+
+
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB):
+    if force or _stale(LIB):
         subprocess.run(["make", "-C", _HERE], check=True, capture_output=True)
     return LIB
 
@@ -48,8 +57,18 @@ _lib = None
 def build_fma() -> str:
     """The oracle compiled with fused multiply-adds allowed (make fma)."""
     path = os.path.join(_HERE, "_build", "libcp_oracle_fma.so")
-    if not os.path.exists(path):
+    if _stale(path):
         subprocess.run(["make", "-C", _HERE, "fma"], check=True, capture_output=True)
+    return path
+
+
+def build_parity() -> str:
+    """The parity build (make parity): pow, the Gateaux factorials and the
+    twin rotation from correctly rounded operations only, the CPU counterpart
+    of the library's reference-order update (cp_options_t.reference_order)."""
+    path = os.path.join(_HERE, "_build", "libcp_oracle_parity.so")
+    if _stale(path):
+        subprocess.run(["make", "-C", _HERE, "parity"], check=True, capture_output=True)
     return path
 
 
@@ -89,6 +108,8 @@ def _load(path) -> C.CDLL:
     L.oracle_pinv_svd.argtypes = [D, C.c_int, D]
     L.oracle_invert.argtypes = [D, C.c_int, D]
     L.oracle_eig_sym3.argtypes = [D, D, D]
+    L.oracle_parity_pow.argtypes = [C.c_double, C.c_double]
+    L.oracle_parity_pow.restype = C.c_double
     return L
 
 

@@ -45,6 +45,8 @@ def units():
         out.append((f"plain_{nt}", "cp_plain_tu.cu", [f"-DCP_TU_NT={nt}", f"-DCP_TU_PMAX={pmax}"]))
     for pmax in (16, 32, 48):
         out.append((f"batch_{pmax}", "cp_batch_tu.cu", [f"-DCP_TU_PMAX={pmax}"]))
+    # the reference-order update: no multiply-add contraction
+    out.append(("ref", "cp_ref_tu.cu", ["-fmad=false"]))
     return [u for u in out if os.path.exists(os.path.join(CSRC, u[1]))]
 
 

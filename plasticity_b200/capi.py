@@ -86,6 +86,7 @@ class CpOptions(C.Structure):
         ("update_variant", C.c_int32),
         ("use_graphs", C.c_int32),
         ("plain_kernel", C.c_int32),
+        ("reference_order", C.c_int32),
     ]
 
 
@@ -168,6 +169,7 @@ def default_options(**kw) -> CpOptions:
     o.update_variant = 0
     o.use_graphs = 1
     o.plain_kernel = 0
+    o.reference_order = 0
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -417,6 +417,9 @@ struct cp_handle {
     double *d_avg_partial = nullptr, *d_avg_out = nullptr;
     int64_t avg_cap = 0;
     double* noalloc_scratch = nullptr;  // device address of g_noalloc_avg_scratch (cp_averages_noalloc)
+    // the reference-order update's per-thread scratch (cp_options_t.reference_order)
+    double* d_refscratch = nullptr;
+    int64_t ref_slot = 0, ref_threads = 0;
     unsigned long long barrier_wait_ns = 0;  // cp_debug_barrier_test: 0 = the default wait
     int barrier_withhold = -1;
     // optional per-launch timing of the update/assembly kernels
@@ -797,8 +800,42 @@ int run_graph(cp_handle* h, const cp_handle::GraphKey& key, Enqueue enqueue) {
     return CP_OK;
 }
 
+// The reference-order update of every group (stream launches): one thread per
+// qp on up to 64 threads per SM, each with a scratch slot of the size the
+// largest lattice needs, allocated on first use and capped at 2 GiB.
+int dispatch_update_ref(cp_handle* h, const double* F, int flag, double F_e, double F_r, double* P, double* T,
+                        double* dPdF, int32_t* st) {
+    if (!h->d_refscratch) {
+        const int64_t slot = ref_scratch_doubles(h->n_max);
+        int64_t threads = (int64_t)h->num_sms * 64;
+        const int64_t cap = (2ll << 30) / (8 * slot);
+        if (threads > cap) threads = cap < 64 ? 64 : cap;
+        void* p = nullptr;
+        if (cudaMalloc(&p, sizeof(double) * slot * threads) != cudaSuccess)
+            return fail(h, CP_E_NOMEM, "reference_order: scratch allocation failed");
+        h->d_refscratch = static_cast<double*>(p);
+        h->ref_slot = slot;
+        h->ref_threads = threads;
+    }
+    double* kF = flag == 0 ? h->d_keepF : nullptr;
+    double* kT = flag == 0 ? h->d_keepT : nullptr;
+    for (size_t gi = 0; gi < h->groups.size(); ++gi) {
+        const auto& g = h->groups[gi];
+        cudaEvent_t ev{};
+        timing_begin(h, (int)gi, &ev);
+        const cudaError_t e = launch_update_ref(h->stream, h->d_lat[g.lattice], h->dopts, g.dev, F, flag, F_e, F_r, P,
+                                                T, dPdF, st, h->d_stats, kF, kT, g.lattice, h->d_refscratch,
+                                                h->ref_slot, h->ref_threads);
+        timing_end(h, (int)gi, ev);
+        if (e != cudaSuccess) return cuda_fail(h, e, "update_ref_kernel");
+    }
+    if (flag == 0) h->have_post = true;
+    return CP_OK;
+}
+
 int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double F_r, double* P, double* T,
                     double* dPdF, int32_t* st) {
+    if (h->opts.reference_order) return dispatch_update_ref(h, F, flag, F_e, F_r, P, T, dPdF, st);
     if (!h->opts.plain_kernel) {
         double* kF = flag == 0 ? h->d_keepF : nullptr;
         double* kT = flag == 0 ? h->d_keepT : nullptr;
@@ -972,6 +1009,7 @@ void cp_destroy(cp_handle* h) {
     cudaFree(h->d_avg_partial);
     cudaFree(h->d_avg_out);
     cudaFree(h->d_tc_err);
+    cudaFree(h->d_refscratch);
     for (auto* d : h->d_lat) cudaFree(d);
     for (auto& p : h->pending) {
         cudaEventDestroy(p.a);
@@ -1086,7 +1124,7 @@ int cp_update(cp_handle* h, const double* h_F, int32_t flag, double F_e, double 
     double* dd = (flag == 1 && h_dPdF) ? h->d_dPdF : nullptr;
     double* dP = h_P ? h->d_P : nullptr;
     double* dT = h_T ? h->d_T : nullptr;
-    if (h->opts.plain_kernel) {
+    if (h->opts.plain_kernel || h->opts.reference_order) {
         CK(h, cudaMemcpyAsync(h->d_F, h_F, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->stream));
         if (int rc = dispatch_update(h, h->d_F, flag, F_e, F_r, dP, dT, dd, h->d_status)) return rc;
         if (h_P) CK(h, cudaMemcpyAsync(h_P, h->d_P, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->stream));
@@ -1172,6 +1210,8 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
     if (!h) return CP_E_ARG;
     if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble: no mesh bound");
     if (!d_U || !d_Ke || !d_Re) return fail(h, CP_E_ARG, "cp_assemble: bad arguments");
+    if (h->opts.reference_order)
+        return fail(h, CP_E_UNSUPPORTED, "cp_assemble: reference_order runs cp_update / cp_update_device only");
     if (int rc = check_device(h)) return rc;
     if (!h->opts.plain_kernel) {
         if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
@@ -1214,6 +1254,8 @@ int cp_assemble_device(cp_handle* h, const double* d_U, double F_e, double F_r, 
 int cp_assemble(cp_handle* h, const double* h_U, double F_e, double F_r, double* h_Ke, double* h_Re,
                 int32_t* h_status) {
     if (!h) return CP_E_ARG;
+    if (h->opts.reference_order)
+        return fail(h, CP_E_UNSUPPORTED, "cp_assemble: reference_order runs cp_update / cp_update_device only");
     if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble: no mesh bound");
     if (!h_U || !h_Ke || !h_Re) return fail(h, CP_E_ARG, "cp_assemble: bad arguments");
     if (int rc = check_device(h)) return rc;
@@ -1293,7 +1335,8 @@ int cp_assemble_mixed_device(cp_handle* h, const double* d_U, double F_e, double
     if (h->n_cells == 0) return fail(h, CP_E_STATE, "cp_assemble_mixed: no mesh bound");
     if (!d_U || !d_Ke || !d_Re) return fail(h, CP_E_ARG, "cp_assemble_mixed: bad arguments");
     if (!h->uniform) return fail(h, CP_E_UNSUPPORTED, "cp_assemble_mixed: needs a uniform mesh (shared gradients)");
-    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_assemble_mixed: needs the sorted update");
+    if (h->opts.plain_kernel || h->opts.reference_order)
+        return fail(h, CP_E_UNSUPPORTED, "cp_assemble_mixed: needs the sorted update");
     if (int rc = check_device(h)) return rc;
     if (!h->d_stage && cudaMalloc(&h->d_stage, sizeof(double) * 90 * h->n_qp) != cudaSuccess)
         return fail(h, CP_E_NOMEM, "cp_assemble_mixed: staging allocation failed");
@@ -2341,7 +2384,7 @@ int cp_update_from_displacement(cp_handle* h, double F_e, double F_r) {
     if (int rc = ensure_staging(h, false)) return rc;
     const int64_t nc = h->n_cells;
     const FromMesh fm{s.d_Ul, h->d_gradN, h->d_JxW, h->uniform};
-    if (h->opts.plain_kernel) {  // F of every qp first, then the plain update on it
+    if (h->opts.plain_kernel || h->opts.reference_order) {  // F of every qp first, then that update on it
         gather_ulocal_kernel<<<blocks_for(24 * nc, SOLVE_BLOCK), SOLVE_BLOCK, 0, h->stream>>>(
             s.d_vec + V_U * s.n_dofs, s.d_cell_dofs, 24 * nc, s.d_Ul);
         mesh_F_kernel<<<blocks_for(h->n_qp, 256), 256, 0, h->stream>>>(fm, h->n_qp, h->d_F);
@@ -2401,7 +2444,8 @@ int cp_autotune(cp_handle* h, const double* d_in, int32_t path, int32_t reps, do
     if (!d_in || (path != CP_TUNE_UPDATE && path != CP_TUNE_ASSEMBLE) || reps < 1 || reps > 64 ||
         !(min_gain >= 0.0 && min_gain < 1.0) || max_results < 0)
         return fail(h, CP_E_ARG, "cp_autotune: bad arguments");
-    if (h->opts.plain_kernel) return fail(h, CP_E_UNSUPPORTED, "cp_autotune: the plain kernel has one launch shape");
+    if (h->opts.plain_kernel || h->opts.reference_order)
+        return fail(h, CP_E_UNSUPPORTED, "cp_autotune: the plain and reference-order updates have one launch shape");
     if (path == CP_TUNE_ASSEMBLE && h->n_cells == 0) return fail(h, CP_E_STATE, "cp_autotune: no mesh bound");
     if (int rc = check_device(h)) return rc;
     if (int rc = ensure_staging(h, path == CP_TUNE_UPDATE)) return rc;
@@ -2543,7 +2587,8 @@ static int batch_run(cp_batch* b, cp_handle* const* hs, int32_t n, const double*
         if (!h) return batch_fail(b, CP_E_ARG, "cp_batch: null handle");
         if (h->device != b->device) return batch_fail(b, CP_E_ARG, "cp_batch: handle on another device");
         if (!h->sys.n_dofs) return batch_fail(b, CP_E_STATE, "cp_batch: a handle has no dofs bound");
-        if (h->opts.plain_kernel) return batch_fail(b, CP_E_UNSUPPORTED, "cp_batch: needs the sorted update");
+        if (h->opts.plain_kernel || h->opts.reference_order)
+            return batch_fail(b, CP_E_UNSUPPORTED, "cp_batch: needs the sorted update");
         for (int j = 0; j < i; ++j)
             if (hs[j] == h) return batch_fail(b, CP_E_ARG, "cp_batch: a handle is listed twice");
     }

@@ -70,6 +70,16 @@ cudaError_t launch_assemble_plain(cudaStream_t s, const LatDev* L, const Opts& o
                                   double F_r, double* Ke, double* Re, int32_t* status, int32_t* stats,
                                   int lattice_id);
 
+// The reference-order update (cp_qpref.cuh, compiled without FMA contraction
+// in cp_ref_tu.cu) of one group, F from a caller array: one thread per qp
+// on at most 'threads' threads, thread t on scratch slot t (scratch holds
+// 'threads' slots of 'slot' doubles).
+int64_t ref_scratch_doubles(int n);
+cudaError_t launch_update_ref(cudaStream_t s, const LatDev* L, const Opts& o, const GroupDev& g, const double* F,
+                              int flag, double F_e, double F_r, double* P, double* T, double* dPdF, int32_t* status,
+                              int32_t* stats, double* keepF, double* keepT, int lattice_id, double* scratch,
+                              int64_t slot, int64_t threads);
+
 // The batched sorted update (update2_batch_kernel) of one lattice class over
 // the groups of several handles, in the class's default launch shape;
 // cp_batch_tu.cu, one translation unit per class.

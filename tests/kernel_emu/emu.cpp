@@ -9,6 +9,7 @@
 #include "../../include/cp_gpu.h"
 #include "../../oracle/cp_oracle.h"
 #include "../../plasticity_b200/csrc/cp_qp2.cuh"
+#include "../../plasticity_b200/csrc/cp_qpref.cuh"
 
 using namespace cp;
 
@@ -47,11 +48,29 @@ void to_aos(const double* s, int64_t n, int w, double* a) {
         for (int c = 0; c < w; ++c) a[i * w + c] = s[c * n + i];
 }
 
-int g_variant = 0;  // 0: qp_update2 (compact), 1: qp_update (plain)
+int g_variant = 0;  // 0: qp_update2 (compact), 1: qp_update (plain), 2: ref::qp_update_ref
 
 template <int NT, int PMAX>
 void run_all(const LatDev& L, const Opts& o, const GroupDev& g, const double* F, int flag, double F_e, double F_r,
              double* P, double* T, double* dPdF, int32_t* stats, int32_t* status) {
+    if (g_variant == 2) {
+#pragma omp parallel
+        {
+            std::vector<double> w((size_t)ref::scratch_doubles(L.n));
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t i = 0; i < g.count; ++i) {
+                QpOut out;
+                out.P = P ? P + 9 * i : nullptr;
+                out.T = T ? T + 9 * i : nullptr;
+                out.dPdF = (dPdF && flag == 1) ? dPdF + 81 * i : nullptr;
+                out.scale = 1.0;
+                const int st = ref::qp_update_ref(L, o, g, i, F + 9 * i, flag, F_e, F_r, out,
+                                                  stats ? stats + 8 * i : nullptr, 0, w.data());
+                if (status) status[i] = st;
+            }
+        }
+        return;
+    }
 #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t i = 0; i < g.count; ++i) {
         M3 Fk;
@@ -73,6 +92,7 @@ void run_all(const LatDev& L, const Opts& o, const GroupDev& g, const double* F,
 }  // namespace
 
 extern "C" void emu_set_variant(int v) { g_variant = v; }
+extern "C" double emu_ref_pow(double x, double y) { return ref::ref_pow(x, y); }
 
 extern "C" int emu_update(const cp_material_t* mat, const cp_options_t* opt, const or_state* st, const double* F,
                           int32_t flag, double F_e, double F_r, double* P, double* T, double* dPdF, int32_t* stats,

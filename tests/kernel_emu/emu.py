@@ -21,6 +21,8 @@ def lib():
         L.emu_update.argtypes = [C.POINTER(CpMaterial), C.POINTER(CpOptions), C.POINTER(O.OrState), D, C.c_int32,
                                  C.c_double, C.c_double, D, D, D, I32, I32, C.c_int32]
         L.emu_lu_compare.argtypes = [D, D, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        L.emu_ref_pow.argtypes = [C.c_double, C.c_double]
+        L.emu_ref_pow.restype = C.c_double
         _lib = L
     return _lib
 
