@@ -252,7 +252,9 @@ def ours(args):
     lid = lattice_ids(n, rank)
     rod = orientations(n, rank)
     mats = materials()
-    h = CpHandle(mats, default_options(device=local))
+    opts = default_options(device=local)
+    opts.update_variant = args.update_variant
+    h = CpHandle(mats, opts)
     h.bind_qps(lid, rod)
     stream = torch.cuda.ExternalStream(h.stream(), device=dev)
 
@@ -1020,6 +1022,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain thread-per-qp kernel")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuning before the timing")
+    ap.add_argument("--update-variant", type=int, default=0,
+                    help="cp_options_t.update_variant: 0 = tuned/default shapes, k forces launch shape k-1")
     ap.add_argument("--no-rve", action="store_true", help="skip the RVE-solve leg")
     ap.add_argument("--no-assembly", action="store_true", help="skip the element-assembly leg")
     ap.add_argument("--asm-n", type=int, default=ASM_N, help="cells per edge of the element-assembly leg's cube")

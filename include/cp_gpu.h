@@ -380,9 +380,15 @@ int cp_update_from_displacement(cp_handle* h, double F_e, double F_r);
 
 /*
  * Launch-shape autotuner of the sorted update (no counterpart in the
- * reference).  Shapes (threads per block / registers per thread):
+ * reference).  Shapes 0-3 run one thread per qp (threads per block /
+ * registers per thread):
  *   0: 256 / 255   1: 256 / 128   2: 64 / 255   3: 64 / 128
- * The untuned rule takes 2 (FCC class) or 3 (BCC/HCP classes) for launches
+ * Shape 4 runs four lanes per qp with the active-set matrix, right-hand
+ * sides and per-system vectors in shared memory, in chunks of qps with one
+ * potentially-active-set size (a persistent grid of two 128-thread blocks
+ * per SM); it serves max_slip_search_iterations = 1 only (otherwise calls
+ * take the untuned rule's shape and the tuner skips it, median -1).  Every
+ * shape gives the same bits.  The untuned rule takes 2 (FCC class) or 3 (BCC/HCP classes) for launches
  * of at most 9,472 qps and 0 or 1 above.  cp_autotune times every shape on
  * the live workload, group by group: path CP_TUNE_UPDATE runs the flag-1
  * update with d_in = F (9*n_qp, device); path CP_TUNE_ASSEMBLE runs the fused
@@ -395,7 +401,7 @@ int cp_update_from_displacement(cp_handle* h, double F_e, double F_r);
  * be NULL) receives one row per lattice group; returns the number of groups
  * or a negative CP_E* code.  Synchronous.
  */
-#define CP_UPDATE_VARIANTS 4
+#define CP_UPDATE_VARIANTS 5
 #define CP_TUNE_UPDATE 0
 #define CP_TUNE_ASSEMBLE 1
 typedef struct cp_tune_result_t {

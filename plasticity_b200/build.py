@@ -30,7 +30,7 @@ NVCC_FLAGS = ARCH + [
     "-I" + os.path.join(ROOT, "include"),
 ]
 
-U2_VARIANTS = 4  # kU2Shapes in csrc/cp_launch.h
+U2_VARIANTS = 4  # thread-per-qp shapes (U2_THREAD_SHAPES in csrc/cp_launch.h)
 
 
 def units():
@@ -41,6 +41,9 @@ def units():
             for v in range(U2_VARIANTS):
                 out.append((f"u2_{pmax}_{fsrc}_{v}", "cp_update_tu.cu",
                             [f"-DCP_TU_PMAX={pmax}", f"-DCP_TU_FSRC={fsrc}", f"-DCP_TU_VARIANT={v}"]))
+    for pmax in (16, 32, 48):
+        for fsrc in ("FromArray", "FromMesh"):
+            out.append((f"quad_{pmax}_{fsrc}", "cp_quad_tu.cu", [f"-DCP_TU_PMAX={pmax}", f"-DCP_TU_FSRC={fsrc}"]))
     for nt, pmax in ((16, 16), (32, 32), (64, 48)):
         out.append((f"plain_{nt}", "cp_plain_tu.cu", [f"-DCP_TU_NT={nt}", f"-DCP_TU_PMAX={pmax}"]))
     for pmax in (16, 32, 48):

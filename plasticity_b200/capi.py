@@ -120,7 +120,7 @@ class CpSolveInfo(C.Structure):
     ]
 
 
-CP_UPDATE_VARIANTS = 4
+CP_UPDATE_VARIANTS = 5
 CP_TUNE_UPDATE = 0
 CP_TUNE_ASSEMBLE = 1
 # launch shapes of the sorted update: (threads per block, registers per thread)

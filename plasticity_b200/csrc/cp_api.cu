@@ -692,8 +692,20 @@ cudaError_t launch_update2_shape(cudaStream_t s, const U2Args& a, const FSrc& fs
         case 0: return launch_update2_v<PMAX, FSrc, 0>(s, a, fs);
         case 1: return launch_update2_v<PMAX, FSrc, 1>(s, a, fs);
         case 2: return launch_update2_v<PMAX, FSrc, 2>(s, a, fs);
-        default: return launch_update2_v<PMAX, FSrc, 3>(s, a, fs);
+        case 3: return launch_update2_v<PMAX, FSrc, 3>(s, a, fs);
+        default: return launch_update4<PMAX, FSrc>(s, a, fs);
     }
+}
+
+// the quad kernels' shared-memory limit, for the current device
+cudaError_t prepare_update4_all() {
+    cudaError_t e = cudaSuccess;
+    const cudaError_t r[6] = {prepare_update4<16, FromArray>(), prepare_update4<32, FromArray>(),
+                              prepare_update4<48, FromArray>(), prepare_update4<16, FromMesh>(),
+                              prepare_update4<32, FromMesh>(),  prepare_update4<48, FromMesh>()};
+    for (cudaError_t x : r)
+        if (x != cudaSuccess) e = x;
+    return e;
 }
 
 // the sorted update of internal qps [i0, i0 + m) of group g (sort done) in
@@ -706,8 +718,9 @@ cudaError_t launch_update2(cp_handle* h, const Group& g, FSrc fs, int64_t i0, in
     if (v < 0 && h->opts.update_variant > 0) v = h->opts.update_variant - 1;
     if (v < 0) v = g.tuned[fsrc_path<FSrc>()];
     if (v < 0) v = u2_default_variant(pmax, m);
+    if (v == U2_QUAD && h->dopts.max_search != 1) v = u2_default_variant(pmax, m);  // one slip-search pass only
     const U2Args a{h->d_lat[g.lattice], h->dopts, g.dev, g.d_perm + i0, m, flag, F_e, F_r, P, T, dPdF, stage, st,
-                   h->d_stats, kF, kT, g.lattice};
+                   h->d_stats, kF, kT, g.lattice, g.d_hist, h->num_sms};
     switch (pmax) {
         case 16: return launch_update2_shape<16>(h->stream, a, fs, v);
         case 32: return launch_update2_shape<32>(h->stream, a, fs, v);
@@ -952,7 +965,8 @@ int cp_create(const cp_material_t* lattices, int32_t n_lattices, const cp_option
         return CP_E_CUDA;
     }
     if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess ||
-        prepare_ke_tc() != cudaSuccess || cudaMalloc(&h->d_tc_err, sizeof(int)) != cudaSuccess ||
+        prepare_ke_tc() != cudaSuccess || prepare_update4_all() != cudaSuccess ||
+        cudaMalloc(&h->d_tc_err, sizeof(int)) != cudaSuccess ||
         cudaMemset(h->d_tc_err, 0, sizeof(int)) != cudaSuccess) {
         cp_destroy(h);
         return CP_E_CUDA;
@@ -2474,6 +2488,7 @@ int cp_autotune(cp_handle* h, const double* d_in, int32_t path, int32_t reps, do
             sort_group(h, g, fm, 0, m);
         std::vector<double> ms(V * reps, -1.0);
         for (int v = 0; v < V && rc == CP_OK; ++v) {
+            if (v == U2_QUAD && h->dopts.max_search != 1) continue;  // not applicable: no timing
             cudaError_t e = launch(v);  // untimed first launch
             for (int r = 0; r < reps && e == cudaSuccess; ++r) {
                 cudaEventRecord(ev[2 * (v * reps + r)], h->stream);

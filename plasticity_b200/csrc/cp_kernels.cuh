@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(QP_BLOCK) assemble_kernel(const LatDev* __rest
             const int ci = d % 3, a = d / 3;
             const double ud = Uc[d];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) F(ci, j) += ud * gq[a * 3 + j];
+            for (int j = 0; j < 3; ++j) F(ci, j) = fmad(ud, gq[a * 3 + j], F(ci, j));
         }
         F(0, 0) += 1.0;
         F(1, 1) += 1.0;
@@ -161,7 +161,7 @@ struct FromMesh {
             const int ci = d % 3, a = d / 3;
             const double ud = Uc[d];
 #pragma unroll
-            for (int j = 0; j < 3; ++j) F(ci, j) += ud * gq[a * 3 + j];
+            for (int j = 0; j < 3; ++j) F(ci, j) = fmad(ud, gq[a * 3 + j], F(ci, j));
         }
         F(0, 0) += 1.0;
         F(1, 1) += 1.0;

@@ -31,6 +31,8 @@ struct U2Args {
     int32_t *status, *stats;
     double *keepF, *keepT;
     int lattice_id;
+    const int* hist;  // the sort's bucket counts, then bucket ends (the quad shape's chunk table)
+    int num_sms;
 };
 
 // Launch shapes of the sorted update (the autotuner's choices): threads per
@@ -40,8 +42,12 @@ struct U2Args {
 struct U2Shape {
     int block, min_blocks;
 };
-constexpr int U2_VARIANTS = 4;
-constexpr U2Shape kU2Shapes[U2_VARIANTS] = {{256, 1}, {256, 2}, {64, 4}, {64, 8}};
+constexpr int U2_THREAD_SHAPES = 4;
+constexpr U2Shape kU2Shapes[U2_THREAD_SHAPES] = {{256, 1}, {256, 2}, {64, 4}, {64, 8}};
+// Shape 4: four lanes per qp with the scratch in shared memory (cp_qp4.cuh,
+// one slip-search pass only).
+constexpr int U2_QUAD = U2_THREAD_SHAPES;
+constexpr int U2_VARIANTS = U2_THREAD_SHAPES + 1;
 
 // Default shape without tuning: launches of at most U2_SPREAD_QPS qps (an
 // RVE's or a served request's group) in 64-thread blocks spread over the SMs,
@@ -57,6 +63,14 @@ inline int u2_default_variant(int pmax, int64_t m) {
 // Sorted update, one translation unit per (PMAX, F source, variant).
 template <int PMAX, class FSrc, int V>
 cudaError_t launch_update2_v(cudaStream_t s, const U2Args& a, const FSrc& fs);
+
+// The quad form of the sorted update (cp_quad_tu.cu, one translation unit per
+// (PMAX, F source)); a.hist and a.num_sms must be set; max_search must be 1.
+// prepare_update4 raises the kernel's shared-memory limit once per device.
+template <int PMAX, class FSrc>
+cudaError_t launch_update4(cudaStream_t s, const U2Args& a, const FSrc& fs);
+template <int PMAX, class FSrc>
+cudaError_t prepare_update4();
 
 // Plain thread-per-qp update (F from a caller array) and plain fused assembly
 // of one group, one translation unit per lattice class.

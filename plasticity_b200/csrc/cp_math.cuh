@@ -32,6 +32,24 @@ using std::atan;
 
 namespace cp {
 
+// Every multiply-add of the helpers below is an explicit fused multiply-add
+// in a fixed order: left to the compiler, a product shared by two
+// expressions (det and inv of one matrix, say) is fused in one kernel and not
+// in another, so the same source would round differently in the plain, sorted
+// and quad forms of the update.  Written out, each helper gives the same bits
+// wherever it is inlined.
+CP_HD double fmad(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+// a0 b0 + a1 b1 + a2 b2 as fma(a2, b2, fma(a1, b1, a0 b0))
+CP_HD double dot3(double a0, double b0, double a1, double b1, double a2, double b2) {
+    return fmad(a2, b2, fmad(a1, b1, a0 * b0));
+}
+
 struct M3 {
     double a[9];
     CP_HD double& operator()(int i, int j) { return a[3 * i + j]; }
@@ -54,7 +72,7 @@ CP_HD M3 mul(const M3& A, const M3& B) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) C(i, j) = A(i, 0) * B(0, j) + A(i, 1) * B(1, j) + A(i, 2) * B(2, j);
+        for (int j = 0; j < 3; ++j) C(i, j) = dot3(A(i, 0), B(0, j), A(i, 1), B(1, j), A(i, 2), B(2, j));
     return C;
 }
 CP_HD M3 mulTN(const M3& A, const M3& B) {  // A^T B
@@ -62,7 +80,7 @@ CP_HD M3 mulTN(const M3& A, const M3& B) {  // A^T B
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) C(i, j) = A(0, i) * B(0, j) + A(1, i) * B(1, j) + A(2, i) * B(2, j);
+        for (int j = 0; j < 3; ++j) C(i, j) = dot3(A(0, i), B(0, j), A(1, i), B(1, j), A(2, i), B(2, j));
     return C;
 }
 CP_HD M3 mulNT(const M3& A, const M3& B) {  // A B^T
@@ -70,7 +88,7 @@ CP_HD M3 mulNT(const M3& A, const M3& B) {  // A B^T
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) C(i, j) = A(i, 0) * B(j, 0) + A(i, 1) * B(j, 1) + A(i, 2) * B(j, 2);
+        for (int j = 0; j < 3; ++j) C(i, j) = dot3(A(i, 0), B(j, 0), A(i, 1), B(j, 1), A(i, 2), B(j, 2));
     return C;
 }
 CP_HD M3 scale(double c, const M3& A) {
@@ -81,7 +99,7 @@ CP_HD M3 scale(double c, const M3& A) {
 }
 CP_HD void axpy(M3& Y, double c, const M3& X) {
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Y.a[i] += c * X.a[i];
+    for (int i = 0; i < 9; ++i) Y.a[i] = fmad(c, X.a[i], Y.a[i]);
 }
 CP_HD M3 sym(const M3& A) {
     M3 S = A;
@@ -93,36 +111,40 @@ CP_HD M3 sym(const M3& A) {
 CP_HD double frob(const M3& A) {
     double s = 0.0;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) s += A.a[i] * A.a[i];
+    for (int i = 0; i < 9; ++i) s = fmad(A.a[i], A.a[i], s);
     return sqrt(s);
 }
 CP_HD double dot9(const M3& A, const M3& B) {
     double s = 0.0;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) s += A.a[i] * B.a[i];
+    for (int i = 0; i < 9; ++i) s = fmad(A.a[i], B.a[i], s);
     return s;
 }
+// a b - c d as fma(a, b, -(c d))
+CP_HD double diff2(double a, double b, double c, double d) { return fmad(a, b, -(c * d)); }
 CP_HD double det(const M3& A) {
-    return A(0, 0) * (A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1)) - A(0, 1) * (A(1, 0) * A(2, 2) - A(1, 2) * A(2, 0)) +
-           A(0, 2) * (A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0));
+    const double m0 = diff2(A(1, 1), A(2, 2), A(1, 2), A(2, 1));
+    const double m1 = diff2(A(1, 0), A(2, 2), A(1, 2), A(2, 0));
+    const double m2 = diff2(A(1, 0), A(2, 1), A(1, 1), A(2, 0));
+    return fmad(A(0, 2), m2, fmad(-A(0, 1), m1, A(0, 0) * m0));
 }
 // inverse by the adjugate, inv = adj(A) * (1/det)
 CP_HD M3 inv(const M3& A) {
-    const double c00 = A(1, 1) * A(2, 2) - A(1, 2) * A(2, 1);
-    const double c01 = A(1, 2) * A(2, 0) - A(1, 0) * A(2, 2);
-    const double c02 = A(1, 0) * A(2, 1) - A(1, 1) * A(2, 0);
-    const double d = A(0, 0) * c00 + A(0, 1) * c01 + A(0, 2) * c02;
+    const double c00 = diff2(A(1, 1), A(2, 2), A(1, 2), A(2, 1));
+    const double c01 = diff2(A(1, 2), A(2, 0), A(1, 0), A(2, 2));
+    const double c02 = diff2(A(1, 0), A(2, 1), A(1, 1), A(2, 0));
+    const double d = dot3(A(0, 0), c00, A(0, 1), c01, A(0, 2), c02);
     const double r = 1.0 / d;
     M3 B;
     B(0, 0) = c00 * r;
     B(1, 0) = c01 * r;
     B(2, 0) = c02 * r;
-    B(0, 1) = (A(0, 2) * A(2, 1) - A(0, 1) * A(2, 2)) * r;
-    B(1, 1) = (A(0, 0) * A(2, 2) - A(0, 2) * A(2, 0)) * r;
-    B(2, 1) = (A(0, 1) * A(2, 0) - A(0, 0) * A(2, 1)) * r;
-    B(0, 2) = (A(0, 1) * A(1, 2) - A(0, 2) * A(1, 1)) * r;
-    B(1, 2) = (A(0, 2) * A(1, 0) - A(0, 0) * A(1, 2)) * r;
-    B(2, 2) = (A(0, 0) * A(1, 1) - A(0, 1) * A(1, 0)) * r;
+    B(0, 1) = diff2(A(0, 2), A(2, 1), A(0, 1), A(2, 2)) * r;
+    B(1, 1) = diff2(A(0, 0), A(2, 2), A(0, 2), A(2, 0)) * r;
+    B(2, 1) = diff2(A(0, 1), A(2, 0), A(0, 0), A(2, 1)) * r;
+    B(0, 2) = diff2(A(0, 1), A(1, 2), A(0, 2), A(1, 1)) * r;
+    B(1, 2) = diff2(A(0, 2), A(1, 0), A(0, 0), A(1, 2)) * r;
+    B(2, 2) = diff2(A(0, 0), A(1, 1), A(0, 1), A(1, 0)) * r;
     return B;
 }
 
@@ -164,7 +186,7 @@ CP_HD M3 voigt_apply(const SymD& D, const M3& X) {
     double w[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-        w[i] = D(i, 0) * v0 + D(i, 1) * v1 + D(i, 2) * v2 + D(i, 3) * v3 + D(i, 4) * v4 + D(i, 5) * v5;
+        w[i] = fmad(D(i, 5), v5, fmad(D(i, 4), v4, fmad(D(i, 3), v3, fmad(D(i, 2), v2, fmad(D(i, 1), v1, D(i, 0) * v0)))));
     M3 A;
     A(0, 0) = w[0];
     A(1, 1) = w[1];
@@ -177,20 +199,20 @@ CP_HD M3 voigt_apply(const SymD& D, const M3& X) {
 
 // odfpoint (rotationOperations.cc:4-51)
 CP_HD M3 odfpoint(double r0, double r1, double r2) {
-    const double rr = r0 * r0 + r1 * r1 + r2 * r2;
+    const double rr = dot3(r0, r0, r1, r1, r2, r2);
     const double t1 = 1.0 - rr, inv2 = 1.0 / (1.0 + rr);
     const double r[3] = {r0, r1, r2};
     M3 R;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) R(i, j) = ((i == j ? t1 : 0.0) + 2.0 * (r[i] * r[j]));
-    R(0, 1) -= 2.0 * r2;
-    R(0, 2) += 2.0 * r1;
-    R(1, 2) -= 2.0 * r0;
-    R(1, 0) += 2.0 * r2;
-    R(2, 0) -= 2.0 * r1;
-    R(2, 1) += 2.0 * r0;
+        for (int j = 0; j < 3; ++j) R(i, j) = fmad(2.0, r[i] * r[j], i == j ? t1 : 0.0);
+    R(0, 1) = fmad(-2.0, r2, R(0, 1));
+    R(0, 2) = fmad(2.0, r1, R(0, 2));
+    R(1, 2) = fmad(-2.0, r0, R(1, 2));
+    R(1, 0) = fmad(2.0, r2, R(1, 0));
+    R(2, 0) = fmad(-2.0, r1, R(2, 0));
+    R(2, 1) = fmad(2.0, r0, R(2, 1));
 #pragma unroll
     for (int i = 0; i < 9; ++i) R.a[i] = R.a[i] * inv2;
     return R;
@@ -215,9 +237,9 @@ CP_HD Sym6 elasticmoduli(const M3& R, const double* __restrict__ C) {
         N[3 + r][0] = R(p, 0) * R(q, 0);
         N[3 + r][1] = R(p, 1) * R(q, 1);
         N[3 + r][2] = R(p, 2) * R(q, 2);
-        N[3 + r][3] = R(p, 1) * R(q, 2) + R(p, 2) * R(q, 1);
-        N[3 + r][4] = R(p, 2) * R(q, 0) + R(p, 0) * R(q, 2);
-        N[3 + r][5] = R(p, 0) * R(q, 1) + R(p, 1) * R(q, 0);
+        N[3 + r][3] = fmad(R(p, 2), R(q, 1), R(p, 1) * R(q, 2));
+        N[3 + r][4] = fmad(R(p, 0), R(q, 2), R(p, 2) * R(q, 0));
+        N[3 + r][5] = fmad(R(p, 1), R(q, 0), R(p, 0) * R(q, 1));
     }
     double T[6][6];
 #pragma unroll
@@ -226,7 +248,7 @@ CP_HD Sym6 elasticmoduli(const M3& R, const double* __restrict__ C) {
         for (int j = 0; j < 6; ++j) {
             double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += N[i][k] * C[6 * k + j];
+            for (int k = 0; k < 6; ++k) s = fmad(N[i][k], C[6 * k + j], s);
             T[i][j] = s;
         }
     Sym6 out;
@@ -237,7 +259,7 @@ CP_HD Sym6 elasticmoduli(const M3& R, const double* __restrict__ C) {
         for (int j = i; j < 6; ++j) {
             double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) s += T[i][k] * N[j][k];
+            for (int k = 0; k < 6; ++k) s = fmad(T[i][k], N[j][k], s);
             out.c[idx++] = s;
         }
     return out;

@@ -99,20 +99,20 @@ __host__ __device__ __forceinline__ void store_soa3(double* __restrict__ f, int6
 __host__ __device__ __forceinline__ double resolved(const LatDev& L, int s, const M3& Xc) {
     const double m0 = ldg(&L.m[3 * s]), m1 = ldg(&L.m[3 * s + 1]), m2 = ldg(&L.m[3 * s + 2]);
     const double n0 = ldg(&L.nn[3 * s]), n1 = ldg(&L.nn[3 * s + 1]), n2 = ldg(&L.nn[3 * s + 2]);
-    const double y0 = Xc(0, 0) * n0 + Xc(0, 1) * n1 + Xc(0, 2) * n2;
-    const double y1 = Xc(1, 0) * n0 + Xc(1, 1) * n1 + Xc(1, 2) * n2;
-    const double y2 = Xc(2, 0) * n0 + Xc(2, 1) * n1 + Xc(2, 2) * n2;
-    return m0 * y0 + m1 * y1 + m2 * y2;
+    const double y0 = dot3(Xc(0, 0), n0, Xc(0, 1), n1, Xc(0, 2), n2);
+    const double y1 = dot3(Xc(1, 0), n0, Xc(1, 1), n1, Xc(1, 2), n2);
+    const double y2 = dot3(Xc(2, 0), n0, Xc(2, 1), n1, Xc(2, 2), n2);
+    return dot3(m0, y0, m1, y1, m2, y2);
 }
 
 // S : X = (R m)^T X (R n) for a Schmid tensor stored as its two vectors
 // v = (R m, R n); the one product form both update kernels use, so that the
 // plain and the sorted kernel round alike
 __host__ __device__ __forceinline__ double schmid_dot(const double* v, const M3& X) {
-    const double y0 = X(0, 0) * v[3] + X(0, 1) * v[4] + X(0, 2) * v[5];
-    const double y1 = X(1, 0) * v[3] + X(1, 1) * v[4] + X(1, 2) * v[5];
-    const double y2 = X(2, 0) * v[3] + X(2, 1) * v[4] + X(2, 2) * v[5];
-    return v[0] * y0 + v[1] * y1 + v[2] * y2;
+    const double y0 = dot3(X(0, 0), v[3], X(0, 1), v[4], X(0, 2), v[5]);
+    const double y1 = dot3(X(1, 0), v[3], X(1, 1), v[4], X(1, 2), v[5]);
+    const double y2 = dot3(X(2, 0), v[3], X(2, 1), v[4], X(2, 2), v[5]);
+    return dot3(v[0], y0, v[1], y1, v[2], y2);
 }
 __host__ __device__ __forceinline__ M3 schmid_of(const double* v) {
     M3 S;
@@ -125,9 +125,38 @@ __host__ __device__ __forceinline__ M3 schmid_of(const double* v) {
 __host__ __device__ __forceinline__ void schmid_vectors(const LatDev& L, int s, const M3& R, double* v) {
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        v[i] = R(i, 0) * ldg(&L.m[3 * s]) + R(i, 1) * ldg(&L.m[3 * s + 1]) + R(i, 2) * ldg(&L.m[3 * s + 2]);
-        v[3 + i] = R(i, 0) * ldg(&L.nn[3 * s]) + R(i, 1) * ldg(&L.nn[3 * s + 1]) + R(i, 2) * ldg(&L.nn[3 * s + 2]);
+        v[i] = dot3(R(i, 0), ldg(&L.m[3 * s]), R(i, 1), ldg(&L.m[3 * s + 1]), R(i, 2), ldg(&L.m[3 * s + 2]));
+        v[3 + i] = dot3(R(i, 0), ldg(&L.nn[3 * s]), R(i, 1), ldg(&L.nn[3 * s + 1]), R(i, 2), ldg(&L.nn[3 * s + 2]));
     }
+}
+
+// New Rodrigues vector of a twin reorientation (rod2quat, quatproduct,
+// quat2rod; updateAfterIncrement.cc:781-821, called at
+// calculatePlasticity.cc:985-1012): the qp's rotation (r0, r1, r2) composed
+// with the 180-degree rotation about twin system sys's normal.
+__host__ __device__ __forceinline__ void twin_rotation(const LatDev& L, int sys, double r0, double r1, double r2,
+                                                       double out[3]) {
+    const double dot = dot3(r0, r0, r1, r1, r2, r2);
+    const double c = cos(atan(sqrt(dot)));
+    const double q2[4] = {c, c * r0, c * r1, c * r2};
+    const double q1[4] = {0.0, ldg(&L.nn[3 * sys]), ldg(&L.nn[3 * sys + 1]), ldg(&L.nn[3 * sys + 2])};
+    const double a = q2[0], b = q1[0];
+    const double d1 = dot3(q1[1], q2[1], q1[2], q2[2], q1[3], q2[3]);
+    double qp0 = fmad(a, b, -d1);
+    double qp1 = fmad(-q1[2], q2[3], fmad(q2[2], q1[3], fmad(b, q2[1], a * q1[1])));
+    double qp2 = fmad(q1[1], q2[3], fmad(-q2[1], q1[3], fmad(b, q2[2], a * q1[2])));
+    double qp3 = fmad(-q1[1], q2[2], fmad(q2[1], q1[2], fmad(b, q2[3], a * q1[3])));
+    if (qp0 < 0) {
+        qp0 = -qp0;
+        qp1 = -qp1;
+        qp2 = -qp2;
+        qp3 = -qp3;
+    }
+    if (fabs(qp0) < 1e-4) qp0 = 1e-4;
+    const double iq = 1 / qp0;
+    out[0] = qp1 * iq;
+    out[1] = qp2 * iq;
+    out[2] = qp3 * iq;
 }
 
 // matrixExponential (matrixOperations.cc:165-186)
@@ -665,27 +694,11 @@ __host__ __device__ int qp_update(const LatDev& L, const Opts& o, const GroupDev
             }
         }
         if (g.twin_c[i] != 1 && F_r > 0 && tmax > F_T) {
-            // rod2quat, quatproduct, quat2rod (updateAfterIncrement.cc:781-821)
-            const double dot = r0 * r0 + r1 * r1 + r2 * r2;
-            const double c = cos(atan(sqrt(dot)));
-            const double q2[4] = {c, c * r0, c * r1, c * r2};
-            const double q1[4] = {0.0, ldg(&L.nn[3 * (ns + pos)]), ldg(&L.nn[3 * (ns + pos) + 1]),
-                                  ldg(&L.nn[3 * (ns + pos) + 2])};
-            double qp[4];
-            const double a = q2[0], b = q1[0];
-            const double d1 = q1[1] * q2[1] + q1[2] * q2[2] + q1[3] * q2[3];
-            qp[0] = (a * b) - d1;
-            qp[1] = a * q1[1] + b * q2[1] + q2[2] * q1[3] - q1[2] * q2[3];
-            qp[2] = a * q1[2] + b * q2[2] - q2[1] * q1[3] + q1[1] * q2[3];
-            qp[3] = a * q1[3] + b * q2[3] + q2[1] * q1[2] - q1[1] * q2[2];
-            if (qp[0] < 0)
-                for (int t = 0; t < 4; ++t) qp[t] = -qp[t];
-            if (fabs(qp[0]) < 1e-4) qp[0] = 1e-4;
-            const double iq = 1 / qp[0];
+            double rr[3];
+            twin_rotation(L, ns + pos, r0, r1, r2, rr);
             for (int t = 0; t < 3; ++t) {
-                const double rr = qp[t + 1] * iq;
-                g.rot_i[(int64_t)t * cnt + i] = rr;
-                g.rotnew_i[(int64_t)t * cnt + i] = rr;
+                g.rot_i[(int64_t)t * cnt + i] = rr[t];
+                g.rotnew_i[(int64_t)t * cnt + i] = rr[t];
             }
             g.twin_i[i] = 1;
             for (int t = 0; t < nw; ++t) g.s_i[(int64_t)(ns + t) * cnt + i] = 100000;

@@ -865,26 +865,11 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             }
         }
         if (g.twin_c[i] != 1 && F_r > 0 && tmax > F_T) {
-            const double dot = r0 * r0 + r1 * r1 + r2 * r2;
-            const double c = cos(atan(sqrt(dot)));
-            const double q2[4] = {c, c * r0, c * r1, c * r2};
-            const double q1[4] = {0.0, ldg(&L.nn[3 * (ns + pos)]), ldg(&L.nn[3 * (ns + pos) + 1]),
-                                  ldg(&L.nn[3 * (ns + pos) + 2])};
-            double qp[4];
-            const double a = q2[0], b = q1[0];
-            const double d1 = q1[1] * q2[1] + q1[2] * q2[2] + q1[3] * q2[3];
-            qp[0] = (a * b) - d1;
-            qp[1] = a * q1[1] + b * q2[1] + q2[2] * q1[3] - q1[2] * q2[3];
-            qp[2] = a * q1[2] + b * q2[2] - q2[1] * q1[3] + q1[1] * q2[3];
-            qp[3] = a * q1[3] + b * q2[3] + q2[1] * q1[2] - q1[1] * q2[2];
-            if (qp[0] < 0)
-                for (int t = 0; t < 4; ++t) qp[t] = -qp[t];
-            if (fabs(qp[0]) < 1e-4) qp[0] = 1e-4;
-            const double iq = 1 / qp[0];
+            double rr[3];
+            twin_rotation(L, ns + pos, r0, r1, r2, rr);
             for (int t = 0; t < 3; ++t) {
-                const double rr = qp[t + 1] * iq;
-                g.rot_i[(int64_t)t * cnt + i] = rr;
-                g.rotnew_i[(int64_t)t * cnt + i] = rr;
+                g.rot_i[(int64_t)t * cnt + i] = rr[t];
+                g.rotnew_i[(int64_t)t * cnt + i] = rr[t];
             }
             g.twin_i[i] = 1;
             for (int t = 0; t < nw; ++t) s_cur[(int64_t)(ns + t) * cnt + i] = 100000;
