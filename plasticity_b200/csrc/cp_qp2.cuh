@@ -30,7 +30,6 @@ namespace cp {
 struct Scratch2 {
     unsigned char *pa0, *cur, *pos;
     double *tau_tr, *b, *h, *x_old, *x, *tn, *kin;
-    double* Sv;   // Schmid tensor of PA system k as S = (R m)(R n)^T: R m, R n (6 per k)
     double* A;    // S_PA of the tangent, 9 rows of leading dimension PMAX
     double* Apa;  // the matrix being solved, leading dimension PMAX
     double* rhs;  // right-hand sides, 9 per row
@@ -379,8 +378,8 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
     constexpr bool kPairLU = PMAX > 32;  // paired elimination steps for the BCC-sized solves
     unsigned char pa0_[PMAX], cur_[PMAX], pos_[PMAX];
     double tau_tr_[PMAX], b_[PMAX], h_[PMAX], x_old_[PMAX], x_[PMAX], tn_[PMAX], kin_[PMAX];
-    double Sv_[PMAX * 6], A_[9 * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
-    const Scratch2 w{pa0_, cur_, pos_, tau_tr_, b_, h_, x_old_, x_, tn_, kin_, Sv_, A_, Apa_, rhs_};
+    double A_[9 * PMAX], Apa_[PMAX * PMAX], rhs_[PMAX * 9];
+    const Scratch2 w{pa0_, cur_, pos_, tau_tr_, b_, h_, x_old_, x_, tn_, kin_, A_, Apa_, rhs_};
     const int n = L.n, ns = L.ns, nw = L.nw;
     const int64_t cnt = g.count;
     int status = 0;
@@ -487,7 +486,6 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         for (int k = 0; k < p_init; ++k) {
             const int a = w.pa0[k];
             w.h[k] = ldg(&L.h0[a]) * pow((1 - s_cur[(int64_t)a * cnt + i] / ldg(&L.ss[a])), ldg(&L.a[a]));
-            schmid_vectors(L, a, R, w.Sv + 6 * k);
             const double Wa = W_cur[(int64_t)a * cnt + i];
             const double kin = ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa;
             const bool ng = (w.tau_tr[k] - Wa) < 0.0;
@@ -498,9 +496,15 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         // columns of its current set straight into the matrix it solves
         // (same expression per entry, so the same values as a stored A).
         // Column j needs M_j = Ce [D2 : sym(Ce S_j)] + 2 sym(Ce S_j) T*; two
-        // columns per pass, so each row's Schmid vectors load once per pair.
+        // columns per pass, so each row's Schmid vectors are formed once per
+        // pair.  The Schmid vectors R m, R n of a PA system are recomputed from
+        // the lattice's constants (read-only, cached on chip) wherever they are
+        // needed rather than kept per thread: the same values each time, and
+        // 6 doubles per PA system less local memory.
         auto column_M = [&](int kj) {
-            const M3 Sj = schmid_of(w.Sv + 6 * kj);
+            double svj[6];
+            schmid_vectors(L, w.pa0[kj], R, svj);
+            const M3 Sj = schmid_of(svj);
             const M3 Y = sym(mul(CE_tr, Sj));
             M3 Mj = mul(CE_tr, voigt_apply(D2, Y));
             axpy(Mj, 2.0, mul(Y, Tst_tr));
@@ -518,8 +522,7 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                     const int ki = w.pos[r];
                     const int asys = w.pa0[ki];
                     double sv[6];
-#pragma unroll
-                    for (int e = 0; e < 6; ++e) sv[e] = w.Sv[6 * ki + e];
+                    schmid_vectors(L, asys, R, sv);
                     const unsigned long long ni = (neg_d >> ki) & 1ull;
                     const double kin = w.kin[ki];
                     const double sm0 = schmid_dot(sv, M0), sm1 = schmid_dot(sv, M1);
@@ -542,7 +545,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 for (int r = 0; r < m; ++r) {
                     const int ki = w.pos[r];
                     const int asys = w.pa0[ki];
-                    const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
+                    double svi[6];
+                    schmid_vectors(L, asys, R, svi);
+                    const double sm = schmid_dot(svi, Mj);
                     double v = ldg(&L.q[asys * NM + bsys]) * hj;
                     v += (((neg_d >> ki) & 1ull) ^ nj) ? -sm : sm;
                     v += w.kin[ki];
@@ -596,7 +601,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 const int a = w.pa0[k];
                 const double sgn =
                     ((w.tau_tr[k] - W_cur[(int64_t)a * cnt + i]) > 0) ? w.x_old[k] : -w.x_old[k];
-                axpy(del_FP, sgn, schmid_of(w.Sv + 6 * k));
+                double svk[6];
+                schmid_vectors(L, a, R, svk);
+                axpy(del_FP, sgn, schmid_of(svk));
             }
             FP_tau = mul(matexp(del_FP, &e_terms, &status), FP_t2);
             FE_tau = mul(F, inv(FP_tau));
@@ -725,7 +732,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 axpy(dtau, 2.0, mul(dE, Tst));
                 for (int r = 0; r < p; ++r) {
                     const int k = w.pos[r];
-                    double v = schmid_dot(w.Sv + 6 * k, dtau);
+                    double svk[6];
+                    schmid_vectors(L, w.pa0[k], R, svk);
+                    double v = schmid_dot(svk, dtau);
                     if (neg_t_bits >> w.pa0[k] & 1ull) v = -v;
                     w.rhs[r * 9 + kl] = v;
                 }
@@ -753,7 +762,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             for (int cj = 0; cj < p; ++cj) {
                 const int kj = w.pos[cj];
                 const int bsys = w.pa0[kj];
-                const M3 Sj = schmid_of(w.Sv + 6 * kj);
+                double svj[6];
+                schmid_vectors(L, bsys, R, svj);
+                const M3 Sj = schmid_of(svj);
                 M3 dm, dp;
                 gateaux_pair(Sj, del_FP, c_terms, dm, dp);
                 const M3 Y = sym(mulTN(dm, X6));
@@ -764,7 +775,9 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                     const int ki = w.pos[ci];
                     const int asys = w.pa0[ki];
                     const bool ni = (neg_t_bits >> asys) & 1ull;
-                    const double sm = schmid_dot(w.Sv + 6 * ki, Mj);
+                    double svi[6];
+                    schmid_vectors(L, asys, R, svi);
+                    const double sm = schmid_dot(svi, Mj);
                     double v = ldg(&L.q[asys * NM + bsys]) * w.h[kj];
                     v += (ni ^ nj) ? -sm : sm;
                     const double Wa = W_cur[(int64_t)asys * cnt + i];
