@@ -441,30 +441,51 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
             P_tau = scale(dFe, mulNT(T_tau, inv(F)));
         }
         // ---- resolved shears, potentially active set (:199-244), compact
+        // (four systems' history loads in flight at a time: a load after a
+        // store to the same arrays would otherwise wait for it)
         nPA = 0;
-        for (int a = 0; a < n; ++a) {
-            double W, sa;
-            if (iter1 == 1) {
-                W = g.W_c[(int64_t)a * cnt + i];
-                sa = g.s_c[(int64_t)a * cnt + i];
-                W_cur[(int64_t)a * cnt + i] = W;
-                s_cur[(int64_t)a * cnt + i] = sa;
-            } else {
-                W = W_cur[(int64_t)a * cnt + i];
-                sa = s_cur[(int64_t)a * cnt + i];
-            }
-            double t = resolved(L, a, tr.Xc);
-            if (a > ns - 1 && (t - W) < 0) t = W;
-            const double bb = fabs(t - W) - sa;
-            if (bb >= tol1) {
-                if (nPA < PMAX) {
-                    w.pa0[nPA] = (unsigned char)a;
-                    w.tau_tr[nPA] = t;
-                    w.b[nPA] = bb;
-                } else {
-                    status |= QP_ACTIVE_OVERFLOW;
+        for (int a0 = 0; a0 < n; a0 += 4) {
+            double Wq[4], sq[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int a = a0 + u;
+                if (a < n) {
+                    if (iter1 == 1) {
+                        Wq[u] = g.W_c[(int64_t)a * cnt + i];
+                        sq[u] = g.s_c[(int64_t)a * cnt + i];
+                    } else {
+                        Wq[u] = W_cur[(int64_t)a * cnt + i];
+                        sq[u] = s_cur[(int64_t)a * cnt + i];
+                    }
                 }
-                ++nPA;
+            }
+            if (iter1 == 1)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int a = a0 + u;
+                    if (a < n) {
+                        W_cur[(int64_t)a * cnt + i] = Wq[u];
+                        s_cur[(int64_t)a * cnt + i] = sq[u];
+                    }
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int a = a0 + u;
+                if (a >= n) continue;
+                const double W = Wq[u], sa = sq[u];
+                double t = resolved(L, a, tr.Xc);
+                if (a > ns - 1 && (t - W) < 0) t = W;
+                const double bb = fabs(t - W) - sa;
+                if (bb >= tol1) {
+                    if (nPA < PMAX) {
+                        w.pa0[nPA] = (unsigned char)a;
+                        w.tau_tr[nPA] = t;
+                        w.b[nPA] = bb;
+                    } else {
+                        status |= QP_ACTIVE_OVERFLOW;
+                    }
+                    ++nPA;
+                }
             }
         }
         if (nPA > PMAX) nPA = PMAX;
@@ -645,22 +666,31 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 }
                 ++nzc;
             }
-            for (int a = 0; a < n; ++a) {
-                double h1 = 0.0;
-                if (nzc <= 4) {
-                    const double* qa = L.q + a * NM;
-                    if (nzc > 0) h1 += ldg(&qa[za0]) * zh0 * zx0;
-                    if (nzc > 1) h1 += ldg(&qa[za1]) * zh1 * zx1;
-                    if (nzc > 2) h1 += ldg(&qa[za2]) * zh2 * zx2;
-                    if (nzc > 3) h1 += ldg(&qa[za3]) * zh3 * zx3;
-                } else {
-                    for (int k = 0; k < p_init; ++k)
-                        if (w.x[k] != 0.0) h1 += ldg(&L.q[a * NM + w.pa0[k]]) * w.h[k] * w.x[k];
+            for (int a0 = 0; a0 < n; a0 += 4) {  // four systems' CRSS loads in flight at a time
+                double sq[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (a0 + u < n) sq[u] = s_cur[(int64_t)(a0 + u) * cnt + i];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int a = a0 + u;
+                    if (a >= n) continue;
+                    double h1 = 0.0;
+                    if (nzc <= 4) {
+                        const double* qa = L.q + a * NM;
+                        if (nzc > 0) h1 += ldg(&qa[za0]) * zh0 * zx0;
+                        if (nzc > 1) h1 += ldg(&qa[za1]) * zh1 * zx1;
+                        if (nzc > 2) h1 += ldg(&qa[za2]) * zh2 * zx2;
+                        if (nzc > 3) h1 += ldg(&qa[za3]) * zh3 * zx3;
+                    } else {
+                        for (int k = 0; k < p_init; ++k)
+                            if (w.x[k] != 0.0) h1 += ldg(&L.q[a * NM + w.pa0[k]]) * w.h[k] * w.x[k];
+                    }
+                    double sv = sq[u] + h1;
+                    const double sat = ldg(&L.ss[a]);
+                    if (sv > sat) sv = sat;
+                    s_cur[(int64_t)a * cnt + i] = sv;
                 }
-                double sv = s_cur[(int64_t)a * cnt + i] + h1;
-                const double sat = ldg(&L.ss[a]);
-                if (sv > sat) sv = sat;
-                s_cur[(int64_t)a * cnt + i] = sv;
             }
             // backstress (:431-436) and b (:438-446) of the PA systems
             for (int k = 0; k < p_init; ++k) {
@@ -681,8 +711,24 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         // ---- fractions (:450-456)
         // Systems outside PA get _conv + 0, PA systems _conv + their total
         // increment (PA members are distinct systems).
-        for (int t = 0; t < nw; ++t) g.tw_i[(int64_t)t * cnt + i] = g.tw_c[(int64_t)t * cnt + i] + 0.0;
-        for (int t = 0; t < ns; ++t) g.sl_i[(int64_t)t * cnt + i] = g.sl_c[(int64_t)t * cnt + i] + 0.0;
+        for (int t0 = 0; t0 < nw; t0 += 4) {  // four loads in flight at a time
+            double c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (t0 + u < nw) c[u] = g.tw_c[(int64_t)(t0 + u) * cnt + i];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (t0 + u < nw) g.tw_i[(int64_t)(t0 + u) * cnt + i] = c[u] + 0.0;
+        }
+        for (int t0 = 0; t0 < ns; t0 += 4) {
+            double c[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (t0 + u < ns) c[u] = g.sl_c[(int64_t)(t0 + u) * cnt + i];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (t0 + u < ns) g.sl_i[(int64_t)(t0 + u) * cnt + i] = c[u] + 0.0;
+        }
         for (int k = 0; k < p_init; ++k) {
             const int a = w.pa0[k];
             if (a < ns)
