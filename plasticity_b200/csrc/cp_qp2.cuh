@@ -443,7 +443,17 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         // ---- resolved shears, potentially active set (:199-244), compact
         // (four systems' history loads in flight at a time: a load after a
         // store to the same arrays would otherwise wait for it)
+        // The row constants of the consistency matrix (:252-306) are formed as
+        // each PA member is found, from the CRSS and backstress in registers:
+        // h_beta in w.h[k]; bit k of neg_d is the sign of tau_tr - W of PA
+        // entry k, w.kin[k] the signed kinematic term of its row (the
+        // reference's sign test di * dj < 0 equals neg_d_i != neg_d_j here,
+        // since |tau_tr - W| >= s + tol > 0 for every PA member).  Bit a of
+        // neg_t_bits is the sign of tau_tr - W at the increment start (the
+        // same W in the first pass).
         nPA = 0;
+        neg_t_bits = 0ull;
+        unsigned long long neg_d = 0ull;
         for (int a0 = 0; a0 < n; a0 += 4) {
             double Wq[4], sq[4];
 #pragma unroll
@@ -478,9 +488,16 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 const double bb = fabs(t - W) - sa;
                 if (bb >= tol1) {
                     if (nPA < PMAX) {
-                        w.pa0[nPA] = (unsigned char)a;
-                        w.tau_tr[nPA] = t;
-                        w.b[nPA] = bb;
+                        const int k = nPA;
+                        w.pa0[k] = (unsigned char)a;
+                        w.tau_tr[k] = t;
+                        w.b[k] = bb;
+                        w.h[k] = ldg(&L.h0[a]) * pow((1 - sa / ldg(&L.ss[a])), ldg(&L.a[a]));
+                        const double kin = ldg(&L.C1[a]) - ldg(&L.C2[a]) * W;
+                        const bool ng = (t - W) < 0.0;
+                        if (ng) neg_d |= (1ull << k);
+                        if (ng && iter1 == 1) neg_t_bits |= (1ull << a);
+                        w.kin[k] = ng ? -kin : kin;
                     } else {
                         status |= QP_ACTIVE_OVERFLOW;
                     }
@@ -492,27 +509,13 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
         if (p0 < 0) p0 = nPA;
         if (nPA == 0) break;
         const int p_init = nPA;
-        neg_t_bits = 0ull;
-        for (int k = 0; k < p_init; ++k) {
-            const int a = w.pa0[k];
-            if ((w.tau_tr[k] - g.W_c[(int64_t)a * cnt + i]) < 0) neg_t_bits |= (1ull << a);
-        }
+        if (iter1 > 1)
+            for (int k = 0; k < p_init; ++k) {
+                const int a = w.pa0[k];
+                if ((w.tau_tr[k] - g.W_c[(int64_t)a * cnt + i]) < 0) neg_t_bits |= (1ull << a);
+            }
 
-        // ---- h_beta (:252-262) and A[PA,PA] (:265-306), packed p_init x p_init
-        // Row constants first: bit k of neg_d is the sign of tau_tr - W of PA
-        // entry k, w.kin[k] the signed kinematic term of its row.  The
-        // reference's sign test di * dj < 0 equals neg_d_i != neg_d_j here,
-        // since |tau_tr - W| >= s + tol > 0 for every PA member.
-        unsigned long long neg_d = 0ull;
-        for (int k = 0; k < p_init; ++k) {
-            const int a = w.pa0[k];
-            w.h[k] = ldg(&L.h0[a]) * pow((1 - s_cur[(int64_t)a * cnt + i] / ldg(&L.ss[a])), ldg(&L.a[a]));
-            const double Wa = W_cur[(int64_t)a * cnt + i];
-            const double kin = ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa;
-            const bool ng = (w.tau_tr[k] - Wa) < 0.0;
-            if (ng) neg_d |= (1ull << k);
-            w.kin[k] = ng ? -kin : kin;
-        }
+        // ---- A[PA,PA] (:265-306), packed p_init x p_init
         // A[PA,PA] is not stored: each removal round builds the rows and
         // columns of its current set straight into the matrix it solves
         // (same expression per entry, so the same values as a stored A).
@@ -693,19 +696,19 @@ __host__ __device__ int qp_update2(const LatDev& L, const Opts& o, const GroupDe
                 }
             }
             // backstress (:431-436) and b (:438-446) of the PA systems
+            // (one pass: each PA system's backstress is read once and its b
+            // formed from the value just computed, the one stored)
             for (int k = 0; k < p_init; ++k) {
                 const int a = w.pa0[k];
-                double& Wa = W_cur[(int64_t)a * cnt + i];
-                if ((w.tau_tr[k] - Wa) > 0)
-                    Wa = Wa + (ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa) * w.x[k];
+                const double W0 = W_cur[(int64_t)a * cnt + i];
+                double Wa;
+                if ((w.tau_tr[k] - W0) > 0)
+                    Wa = W0 + (ldg(&L.C1[a]) - ldg(&L.C2[a]) * W0) * w.x[k];
                 else
-                    Wa = Wa + (-ldg(&L.C1[a]) - ldg(&L.C2[a]) * Wa) * w.x[k];
+                    Wa = W0 + (-ldg(&L.C1[a]) - ldg(&L.C2[a]) * W0) * w.x[k];
+                W_cur[(int64_t)a * cnt + i] = Wa;
+                if (w.cur[k]) w.b[k] = fabs(w.tn[k] - Wa) - s_cur[(int64_t)a * cnt + i];
             }
-            for (int k = 0; k < p_init; ++k)
-                if (w.cur[k]) {
-                    const int a = w.pa0[k];
-                    w.b[k] = fabs(w.tn[k] - W_cur[(int64_t)a * cnt + i]) - s_cur[(int64_t)a * cnt + i];
-                }
         }
 
         // ---- fractions (:450-456)
