@@ -389,7 +389,7 @@ int cp_update_from_displacement(cp_handle* h, double F_e, double F_r);
  * per SM); it serves max_slip_search_iterations = 1 only (otherwise calls
  * take the untuned rule's shape and the tuner skips it, median -1).  Every
  * shape gives the same bits.  The untuned rule takes 2 (FCC class) or 3 (BCC/HCP classes) for launches
- * of at most 9,472 qps and 0 or 1 above.  cp_autotune times every shape on
+ * of at most 9,472 qps and 0 above.  cp_autotune times every shape on
  * the live workload, group by group: path CP_TUNE_UPDATE runs the flag-1
  * update with d_in = F (9*n_qp, device); path CP_TUNE_ASSEMBLE runs the fused
  * assembly's update with d_in = U_local (24*n_cells, device).  Each shape

@@ -50,14 +50,16 @@ constexpr int U2_QUAD = U2_THREAD_SHAPES;
 constexpr int U2_VARIANTS = U2_THREAD_SHAPES + 1;
 
 // Default shape without tuning: launches of at most U2_SPREAD_QPS qps (an
-// RVE's or a served request's group) in 64-thread blocks spread over the SMs,
-// larger ones in 256-thread blocks; 255 registers for the FCC class (PMAX 16),
-// 128 for the BCC/HCP classes (measured per class).
+// RVE's or a served request's group) in 64-thread blocks spread over the SMs
+// (255 registers for the FCC class, PMAX 16; 128 for the BCC/HCP classes),
+// larger ones in 256-thread blocks of 255 registers, one per SM (measured per
+// class on the 2^21-qp mixed workload: BCC 11.7 against 13.1 ms for two
+// 128-register blocks per SM, FCC 6.6 against 8.5, HCP 2.26 against 2.27).
 constexpr int64_t U2_SPREAD_QPS = 148 * 64;
 inline int u2_default_variant(int pmax, int64_t m) {
     const bool small_class = pmax <= 16;
     if (m <= U2_SPREAD_QPS) return small_class ? 2 : 3;
-    return small_class ? 0 : 1;
+    return 0;
 }
 
 // Sorted update, one translation unit per (PMAX, F source, variant).
