@@ -45,9 +45,10 @@ PRIOR_STEPS = 10
 AMP = 2e-4
 METRIC = "qp-updates/s (calculatePlasticity + dP/dF, FP64)"
 # DRAM bytes (read + write) per qp of the sorted update, per lattice class,
-# from ncu --set full --clock-control none -k regex:update2 on the 2^18-qp
-# case (python bench.py --n-qp 262144 --steps 1 --warmup 3 with every leg off)
-NCU_DRAM_BYTES_PER_QP = {"fcc": 8597.1, "bcc": 37983.0, "hcp": 7520.4}
+# from ncu --set full --clock-control none -k regex:update2 -s 30 -c 3 on the
+# 2^18-qp case (python bench.py --n-qp 262144 --steps 1 --warmup 1 --no-tune
+# with every leg off), the untuned default shape
+NCU_DRAM_BYTES_PER_QP = {"fcc": 8698.1, "bcc": 32611.0, "hcp": 6377.1}
 
 
 # --------------------------------------------------------------------- workload
