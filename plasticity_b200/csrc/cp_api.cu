@@ -153,11 +153,14 @@ __global__ void __launch_bounds__(AVG_BLOCK)
                             const double* __restrict__ keepT, const double* __restrict__ JxW, int uniform,
                             double* __restrict__ partial) {
     __shared__ double red[AVG_BLOCK / 32][AVG_N];
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // qps in bind order (the group's j-th bound qp), so the sums do not depend
+    // on the internal order of the history
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double v[AVG_N];
 #pragma unroll
     for (int c = 0; c < AVG_N; ++c) v[c] = 0.0;
-    if (i < g.count) {
+    if (j < g.count) {
+        const int64_t i = g.where ? g.where[j] : j;
         const int64_t cnt = g.count;
         const int64_t k = g.qp[i];
         const double w = uniform ? JxW[k & 7] : JxW[k];
@@ -338,10 +341,15 @@ struct Group {
     unsigned char* d_key = nullptr;  // sort key per internal qp
     int* d_perm = nullptr;           // internal qps in sorted order
     int* d_hist = nullptr;           // SORT_BUCKETS counts, then SORT_BUCKETS offsets
+    int64_t* d_qp_tmp = nullptr;     // the reordered qp map before it replaces d_qp
+    int* d_where = nullptr;          // internal index of the qp bound j-th (identity until reordered)
+    mutable bool sorted = false;     // d_key holds the keys of a sort since the last reorder
     int tuned[2] = {-1, -1};         // launch shape chosen by cp_autotune (F from an array / from the
                                      // mesh); -1: the default rule of u2_default_variant
     GroupDev dev{};
-    std::vector<int64_t> qp_host;    // host copy of d_qp (increasing caller indices)
+    std::vector<int64_t> qp_host;    // the group's caller indices in bind order (increasing): the
+                                     // internal order of the sorted pipeline differs only within
+                                     // the reorder segments, so chunk bounds still follow from it
 };
 
 // Host-pointer updates run in caller-order chunks so that one chunk's copies
@@ -498,6 +506,8 @@ void free_group(Group& g) {
     cudaFree(g.d_key);
     cudaFree(g.d_perm);
     cudaFree(g.d_hist);
+    cudaFree(g.d_qp_tmp);
+    cudaFree(g.d_where);
     g = Group{};
 }
 
@@ -618,6 +628,7 @@ void carve(Group& g) {
     d.sl_i = take(g.ns);
     d.twin_c = g.d_twin;
     d.twin_i = g.d_twin + c;
+    d.where = g.d_where;
 }
 
 unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -674,6 +685,7 @@ void timing_end(cp_handle* h, int gi, cudaEvent_t a) {
 template <class FSrc>
 void sort_group(cp_handle* h, const Group& g, FSrc fs, int64_t i0, int64_t m) {
     cudaMemsetAsync(g.d_hist, 0, sizeof(int) * SORT_BUCKETS, h->stream);
+    g.sorted = true;
     classify_kernel<FSrc><<<blocks_for(m, QP_BLOCK), QP_BLOCK, 0, h->stream>>>(h->d_lat[g.lattice], h->dopts, g.dev,
                                                                              fs, i0, m, g.d_key, g.d_hist);
     bucket_scan_kernel<<<1, 32, 0, h->stream>>>(g.d_hist, g.d_hist + SORT_BUCKETS);
@@ -810,6 +822,9 @@ int run_graph(cp_handle* h, const cp_handle::GraphKey& key, Enqueue enqueue) {
     hit->last_use = ++h->graph_clock;
     CK(h, cudaGraphLaunch(hit->exec, h->stream));
     ++h->graph_launches;
+    // every graph of this handle runs the sort of every lattice group, so the
+    // keys of a replay are those of this call
+    for (const auto& g : h->groups) g.sorted = true;
     return CP_OK;
 }
 
@@ -890,6 +905,104 @@ int dispatch_update(cp_handle* h, const double* F, int flag, double F_e, double 
 int check_device(cp_handle* h) {
     CK(h, cudaSetDevice(h->device));
     return CP_OK;
+}
+
+// ---------------------------------------------------------------- history order
+// The sorted update reads each qp's history (structure of arrays, component c
+// of internal qp i at c * count + i) at the internal indices of its sort
+// order; when the internal order is the sort order, a warp's 32 qps are 32
+// neighbouring indices and every history access coalesces, instead of one
+// 32-byte sector per 8-byte value.  So cp_commit, which copies the _iter half
+// over the _conv half anyway, also permutes each group's history (both
+// halves), twin flags and qp map into the order of the keys of the last sort:
+// a stable counting sort by key within each reorder segment.  The segments are
+// bounded by every internal index at which a caller-order chunk of the host
+// calls starts, so each chunk keeps its contiguous internal range.  Every
+// kernel addresses the history by internal index and maps to the caller by
+// qp[i], so no result changes.
+
+// Stable counting sort by key of internal qps [seg[b], seg[b + 1]) (one block
+// per segment, tiles of 256 in order): src[p] is the internal qp that moves to
+// position p.
+__global__ void __launch_bounds__(256) reorder_sort_kernel(const unsigned char* __restrict__ key,
+                                                           const int* __restrict__ seg, int* __restrict__ src) {
+    __shared__ int base[SORT_BUCKETS];
+    __shared__ int wcnt[8][SORT_BUCKETS];
+    const int lo = seg[blockIdx.x], hi = seg[blockIdx.x + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < SORT_BUCKETS) base[tid] = 0;
+    __syncthreads();
+    for (int i = lo + tid; i < hi; i += 256) atomicAdd(&base[key[i] < SORT_BUCKETS ? key[i] : SORT_BUCKETS - 1], 1);
+    __syncthreads();
+    if (tid == 0) {
+        int acc = lo;
+        for (int b = 0; b < SORT_BUCKETS; ++b) {
+            const int c = base[b];
+            base[b] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    for (int t0 = lo; t0 < hi; t0 += 256) {
+        const int i = t0 + tid;
+        const bool valid = i < hi;
+        const int k = valid ? (key[i] < SORT_BUCKETS ? key[i] : SORT_BUCKETS - 1) : SORT_BUCKETS;
+        for (int e = tid; e < 8 * SORT_BUCKETS; e += 256) (&wcnt[0][0])[e] = 0;
+        __syncthreads();
+        const unsigned same = __match_any_sync(0xffffffffu, k);
+        const int rank = __popc(same & ((1u << lane) - 1u));
+        if (valid && lane == __ffs(same) - 1) wcnt[warp][k] = __popc(same);
+        __syncthreads();
+        if (valid) {
+            int off = base[k] + rank;
+            for (int w = 0; w < warp; ++w) off += wcnt[w][k];
+            src[off] = i;
+        }
+        __syncthreads();
+        if (tid < SORT_BUCKETS) {
+            int sum = 0;
+            for (int w = 0; w < 8; ++w) sum += wcnt[w][tid];
+            base[tid] += sum;
+        }
+        __syncthreads();
+    }
+}
+
+// dst[r * count + p] = srcv[r * count + src[p]] for every row r of a field block
+template <class T>
+__global__ void reorder_gather_kernel(const T* __restrict__ srcv, T* __restrict__ dst, int64_t rows, int64_t count,
+                                      const int* __restrict__ src) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const int64_t from = src[p];
+    for (int64_t r = 0; r < rows; ++r) dst[r * count + p] = srcv[r * count + from];
+}
+
+// inv[src[p]] = p: the new position of every old internal index ...
+__global__ void reorder_inverse_kernel(const int* __restrict__ src, int64_t count, int* __restrict__ inv) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < count) inv[src[p]] = (int)p;
+}
+// ... and where[j] <- inv[where[j]] (a second launch, after the inverse is whole)
+__global__ void reorder_where_kernel(const int* __restrict__ inv, int64_t count, int* __restrict__ where) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < count) where[j] = inv[where[j]];
+}
+
+// The internal indices at which reorder segments of group g start (with 0 and
+// count): every start of a caller-order chunk of qps or of cells.
+std::vector<int> reorder_segments(const cp_handle* h, const Group& g) {
+    std::vector<int64_t> b{0, g.count};
+    const auto& q = g.qp_host;
+    const int cq = chunks_for(h->n_qp);
+    for (int c = 1; c < cq; ++c)
+        b.push_back(std::lower_bound(q.begin(), q.end(), h->n_qp * c / cq) - q.begin());
+    if (h->n_cells > 0)
+        for (int c = 1; c < cq; ++c)
+            b.push_back(std::lower_bound(q.begin(), q.end(), 8 * (h->n_cells * c / cq)) - q.begin());
+    std::sort(b.begin(), b.end());
+    b.erase(std::unique(b.begin(), b.end()), b.end());
+    return std::vector<int>(b.begin(), b.end());
 }
 
 }  // namespace
@@ -1076,13 +1189,21 @@ int cp_bind_qps(cp_handle* h, int64_t n_qp, const int32_t* lattice_id, const dou
             cudaMalloc(&g.d_twin, sizeof(int) * 2 * g.count) != cudaSuccess ||
             cudaMalloc(&g.d_key, g.count) != cudaSuccess ||
             cudaMalloc(&g.d_perm, sizeof(int) * g.count) != cudaSuccess ||
-            cudaMalloc(&g.d_hist, sizeof(int) * 2 * SORT_BUCKETS) != cudaSuccess) {
+            cudaMalloc(&g.d_hist, sizeof(int) * 2 * SORT_BUCKETS) != cudaSuccess ||
+            cudaMalloc(&g.d_qp_tmp, sizeof(int64_t) * g.count) != cudaSuccess ||
+            cudaMalloc(&g.d_where, sizeof(int) * g.count) != cudaSuccess ||
+            cudaMemset(g.d_key, 0, g.count) != cudaSuccess) {
             free_group(g);
             cudaFree(d_rod);
             free_qps(h);
             return fail(h, CP_E_NOMEM, "cp_bind_qps: device allocation failed");
         }
         CK(h, cudaMemcpy(g.d_qp, idx[l].data(), sizeof(int64_t) * g.count, cudaMemcpyHostToDevice));
+        {
+            std::vector<int> iota((size_t)g.count);
+            for (int64_t j = 0; j < g.count; ++j) iota[(size_t)j] = (int)j;
+            CK(h, cudaMemcpy(g.d_where, iota.data(), sizeof(int) * g.count, cudaMemcpyHostToDevice));
+        }
         g.qp_host = idx[l];
         carve(g);
         init_state_kernel<<<blocks_for(g.count, 256), 256, 0, h->stream>>>(h->d_lat[l], g.dev, d_rod);
@@ -1492,9 +1613,38 @@ int cp_commit(cp_handle* h) {
     if (!h) return CP_E_ARG;
     if (h->n_qp == 0) return fail(h, CP_E_STATE, "cp_commit: no qps bound");
     if (int rc = check_device(h)) return rc;
+    const bool reorder = !h->opts.plain_kernel && !h->opts.reference_order;
     for (const auto& g : h->groups) {
         // the _iter half of the block directly follows the _conv half
         const int64_t half = group_doubles(g.n, g.ns, g.nw, g.count) / 2;
+        if (reorder && g.sorted) {
+            // _conv in the order of the last sort's keys, gathered from _iter
+            // (the sort's permutation buffer holds the source indices), then
+            // _iter, the twin flags and the qp map the same
+            const std::vector<int> seg = reorder_segments(h, g);
+            const int nseg = (int)seg.size() - 1;
+            CK(h, cudaMemcpyAsync(g.d_hist, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice, h->stream));
+            reorder_sort_kernel<<<nseg, 256, 0, h->stream>>>(g.d_key, g.d_hist, g.d_perm);
+            const unsigned nb = blocks_for(g.count, 256);
+            reorder_gather_kernel<double><<<nb, 256, 0, h->stream>>>(g.d_block + half, g.d_block, half / g.count,
+                                                                     g.count, g.d_perm);
+            reorder_gather_kernel<int><<<nb, 256, 0, h->stream>>>(g.d_twin + g.count, g.d_twin, 1, g.count,
+                                                                  g.d_perm);
+            reorder_gather_kernel<int64_t><<<nb, 256, 0, h->stream>>>(g.d_qp, g.d_qp_tmp, 1, g.count, g.d_perm);
+            CK(h, cudaGetLastError());
+            CK(h, cudaMemcpyAsync(g.d_block + half, g.d_block, sizeof(double) * half, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+            CK(h, cudaMemcpyAsync(g.d_twin + g.count, g.d_twin, sizeof(int) * g.count, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+            CK(h, cudaMemcpyAsync(g.d_qp, g.d_qp_tmp, sizeof(int64_t) * g.count, cudaMemcpyDeviceToDevice,
+                                  h->stream));
+            int* inv = reinterpret_cast<int*>(g.d_qp_tmp);  // new position of each old internal index
+            reorder_inverse_kernel<<<nb, 256, 0, h->stream>>>(g.d_perm, g.count, inv);
+            reorder_where_kernel<<<nb, 256, 0, h->stream>>>(inv, g.count, g.d_where);
+            CK(h, cudaGetLastError());
+            g.sorted = false;
+            continue;
+        }
         CK(h, cudaMemcpyAsync(g.d_block, g.d_block + half, sizeof(double) * half, cudaMemcpyDeviceToDevice,
                               h->stream));
         CK(h, cudaMemcpyAsync(g.d_twin, g.d_twin + g.count, sizeof(int) * g.count, cudaMemcpyDeviceToDevice,
@@ -2638,6 +2788,7 @@ static int batch_run(cp_batch* b, cp_handle* const* hs, int32_t n, const double*
             d.g = g.dev;
             d.fm = fm;
             d.key = g.d_key;
+            g.sorted = true;
             d.hist = g.d_hist;
             d.perm = g.d_perm;
             d.m = g.count;

@@ -67,6 +67,7 @@ struct GroupDev {
     int* twin_c;
     double *Fp_i, *Fe_i, *s_i, *W_i, *rot_i, *rotnew_i, *tw_i, *sl_i;
     int* twin_i;
+    const int* where;  // internal index of the qp bound j-th in the group (null: j itself)
 };
 
 struct QpOut {

@@ -129,6 +129,7 @@ extern "C" int emu_update(const cp_material_t* mat, const cp_options_t* opt, con
     for (int k = 0; k < 16; ++k) *slots[k] = fields[k].soa.data();
     g.twin_c = twin_c.data();
     g.twin_i = twin_i.data();
+    g.where = nullptr;
     if (nT <= 16)
         run_all<16, 16>(L, o, g, F, flag, F_e, F_r, P, T, dPdF, stats, status);
     else if (nT <= 32)

@@ -178,3 +178,36 @@ def test_autotune_assembly_path(cuda_lib):
     _same(K1, K0, "Ke after tuning")
     _same(R1, R0, "Re after tuning")
     be.close()
+
+
+def test_reordered_history_gives_the_same_bits(cuda_lib):
+    """cp_commit permutes a sorted handle's history into the order of its last
+    sort (the plain handle keeps bind order).  Over several committed
+    increments of the host call, which at this size runs in two caller-order
+    chunks (of qps and, for the mesh-bound calls, of cells: the reorder keeps
+    within the segments they bound), P, dP/dF, status, statistics, every
+    history field in caller order and the volume averages stay the plain
+    drop-in's bits."""
+    n = (1 << 18) + 4096
+    rng = np.random.default_rng(23)
+    lid = np.repeat(rng.choice(3, size=n // 8, p=[0.5, 0.3, 0.2]), 8).astype(np.int32)  # one lattice per cell
+    rod = M.random_rodrigues(rng, n)
+    mats = [M.fcc_cu(), M.bcc_48(), M.hcp_mg()]
+    hs = CpHandle(mats, default_options())
+    hp = CpHandle(mats, default_options(plain_kernel=1))
+    cell = H.StructuredMesh((1, 1, 1))  # every cell the unit cube's (the averages weigh by JxW)
+    for h in (hs, hp):
+        h.bind_qps(lid, rod)
+        h.bind_mesh(n // 8, cell.grad_N, cell.JxW, True)
+    F = np.tile(np.eye(3).ravel(), (n, 1))
+    for inc in range(4):
+        F = (F.reshape(-1, 3, 3) @ (np.eye(3) + 3e-4 * rng.standard_normal((n, 3, 3)))).reshape(-1, 9)
+        _assert_same_update(hs, hp, F, 1)
+        _assert_same_update(hs, hp, F, 0)
+        _same(hs.averages(), hp.averages(), f"averages (increment {inc})")
+        for h in (hs, hp):
+            h.commit()
+        for f in STATE_FIELDS:
+            _same(hs.get_state(f + "_conv"), hp.get_state(f + "_conv"), f + "_conv")
+    for h in (hs, hp):
+        h.close()
