@@ -264,7 +264,11 @@ int cp_averages_noalloc(cp_handle* h, double out[22]);
 /* reorient() (reorient.cc:4-98) on all qps: updates rotnew_conv. */
 int cp_reorient(cp_handle* h);
 
-/* Commit the increment: *_conv = *_iter (updateAfterIncrement.cc:287-305). */
+/* Commit the increment: *_conv = *_iter (updateAfterIncrement.cc:287-305).
+ * In the sorted pipeline (not plain_kernel, not reference_order) the device
+ * storage of each lattice group is also permuted into the order of the last
+ * update's sort keys (within the chunks of the host-pointer calls); caller
+ * order, cp_get_state / cp_set_state and every result are unchanged. */
 int cp_commit(cp_handle* h);
 
 /* History fields for cp_get_state / cp_set_state.  Per-qp widths: */
