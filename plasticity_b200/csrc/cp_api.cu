@@ -2312,7 +2312,9 @@ int mixed_newton_iteration(cp_handle* h, const cp_solver_t& sv, const double* h_
             CK(h, cudaMemsetAsync(s.d_info, 0, sizeof(int) * 3, h->stream));
             CK(h, cudaMemsetAsync(s.d_sc, 0, sizeof(double) * SC_COUNT, h->stream));
             CK(h, cudaMemsetAsync(s.d_ticket, 0, sizeof(unsigned int) * 8, h->stream));
-            norm2_f32_kernel<<<RED_BLOCKS, SOLVE_BLOCK, 0, h->stream>>>(w(MV_R), n, s.d_sc, SC_BB, s.d_fpartial,
+            // (RED_BLOCKS partials: the RED_BLOCKS-sized buffer, not the fused
+            // iteration's n / 8 + 64, which smaller systems would overrun)
+            norm2_f32_kernel<<<RED_BLOCKS, SOLVE_BLOCK, 0, h->stream>>>(w(MV_R), n, s.d_sc, SC_BB, s.d_partial,
                                                                         s.d_ticket + 3);
             int queued = 0;
             const int* done = s.d_done;
