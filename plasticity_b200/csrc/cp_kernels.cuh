@@ -275,11 +275,26 @@ __global__ void __launch_bounds__(256) bucket_scatter_kernel(const unsigned char
 // non-null 'stage' (the assembly path) JxW*P and JxW*dP/dF go to stage[90k..].
 // Threads run the qps in sorted order (descending potentially-active-set
 // size): consecutive threads, and so the lanes of a warp, run solves of
-// similar size.  (Interleaving large- and small-solve warps across SMs,
-// sorting only inside 256-qp blocks, and a persistent grid-stride launch with
-// 64-256 resident threads per SM all measured slower.)  The launch shape
-// (threads per block, registers per thread) is a template choice, see
-// kU2Shapes in cp_launch.h.
+// similar size.  (Mixing large- and small-solve warps inside a block, sorting
+// only inside 256-qp blocks, and a persistent grid-stride launch with 64-256
+// resident threads per SM all measured slower.)  The launch shape (threads
+// per block, registers per thread) is a template choice, see kU2Shapes in
+// cp_launch.h.
+//
+// Block order: for the classes of at most 32 systems the blocks take the sorted
+// ranges alternately from the two ends (block 2b the b-th range from the
+// largest solves, block 2b+1 the b-th from the smallest), so the SMs hold a mix
+// of large and small solves and their per-thread scratch shares the L2 with
+// less spilling to DRAM (2^21-qp mixed workload: FCC 6.79 -> 6.63 ms, HCP 2.24
+// -> 1.90 ms).  The 48-system class keeps the ranges in descending order: its
+// largest solves are long enough that taking them first shortens the tail more
+// (interleaved 11.94 against 11.69 ms).  Each qp's update is independent of
+// which block runs it, so the order changes no result.
+template <int PMAX>
+__device__ __forceinline__ int64_t update2_block_range(int64_t b, int64_t nb) {
+    if (PMAX > 32) return b;
+    return (b & 1) ? nb - 1 - (b >> 1) : (b >> 1);
+}
 template <int PMAX, class FSrc>
 __device__ __forceinline__ void update2_one(const LatDev& L, const Opts& o, const GroupDev& g, const FSrc& fs,
                                             int64_t i, int flag, double F_e, double F_r, double* __restrict__ P,
@@ -325,7 +340,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                    double* __restrict__ keepF, double* __restrict__ keepT, int lattice_id) {
     // per-thread rotated-stiffness slots, entry e of thread t at sD2[e * BLOCK + t]
     __shared__ double sD2[21 * BLOCK];
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j = update2_block_range<PMAX>(blockIdx.x, gridDim.x) * blockDim.x + threadIdx.x;
     if (j < m)
         update2_one<PMAX>(*L, o, g, fs, perm[j], flag, F_e, F_r, P, T, dPdF, stage, status, stats, keepF, keepT,
                           lattice_id, sD2 + threadIdx.x, BLOCK);
