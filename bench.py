@@ -48,7 +48,7 @@ METRIC = "qp-updates/s (calculatePlasticity + dP/dF, FP64)"
 # from ncu --set full --clock-control none -k regex:update2 -s 30 -c 3 on the
 # 2^18-qp case (python bench.py --n-qp 262144 --steps 1 --warmup 1 --no-tune
 # with every leg off), the untuned default shape
-NCU_DRAM_BYTES_PER_QP = {"fcc": 8698.1, "bcc": 32611.0, "hcp": 6377.1}
+NCU_DRAM_BYTES_PER_QP = {"fcc": 8957.8, "bcc": 32006.4, "hcp": 5758.1}
 
 
 # --------------------------------------------------------------------- workload
