@@ -2249,11 +2249,19 @@ int mixed_newton_iteration(cp_handle* h, const cp_solver_t& sv, const double* h_
                            cp_solve_info_t* info) {
     auto& s = h->sys;
     const int64_t n = s.n_dofs, nc = h->n_cells;
-    if (!s.d_vals32 &&
-        (cudaMalloc(&s.d_vals32, sizeof(float) * s.nnz) != cudaSuccess ||
-         cudaMalloc(&s.d_valsT32, sizeof(float) * s.nnz) != cudaSuccess ||
-         cudaMalloc(&s.d_vec32, sizeof(float) * MV_COUNT * n) != cudaSuccess))
-        return fail(h, CP_E_NOMEM, "cp_newton_iteration: mixed-precision buffers");
+    if (!s.d_vals32) {
+        if (cudaMalloc(&s.d_vals32, sizeof(float) * s.nnz) != cudaSuccess ||
+            cudaMalloc(&s.d_valsT32, sizeof(float) * s.nnz) != cudaSuccess ||
+            cudaMalloc(&s.d_vec32, sizeof(float) * MV_COUNT * n) != cudaSuccess) {
+            cudaFree(s.d_vals32);
+            cudaFree(s.d_valsT32);
+            cudaFree(s.d_vec32);
+            s.d_vals32 = s.d_valsT32 = s.d_vec32 = nullptr;
+            return fail(h, CP_E_NOMEM, "cp_newton_iteration: mixed-precision buffers");
+        }
+        // the FP32 vectors start as zeros, like the FP64 ones of cp_bind_dofs
+        CK(h, cudaMemsetAsync(s.d_vec32, 0, sizeof(float) * MV_COUNT * n, h->stream));
+    }
     double* V = s.d_vec;
     auto v = [&](int k) { return V + (int64_t)k * n; };
     auto w = [&](int k) { return s.d_vec32 + (int64_t)k * n; };

@@ -387,8 +387,10 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) fbicg_dir_kernel(
     const double beta = first ? 0.0 : rho / sc[SC_RHO_OLD];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    p[i] = z[i] + beta * p[i];
-    pt[i] = zt[i] + beta * pt[i];
+    // the first direction is z itself, as in the persistent solve: the old p
+    // is not read (a solve that broke down may have left non-finite values)
+    p[i] = first ? z[i] : z[i] + beta * p[i];
+    pt[i] = first ? zt[i] : zt[i] + beta * pt[i];
 }
 
 // (3) q = K p and q~ = K^T p~ (a warp per row, both in one pass over the

@@ -148,8 +148,10 @@ __global__ void __launch_bounds__(SOLVE_BLOCK) mbicg_dir_kernel(
     const float beta = first ? 0.0f : (float)(rho / sc[SC_RHO_OLD]);
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    p[i] = z[i] + beta * p[i];
-    pt[i] = zt[i] + beta * pt[i];
+    // the first direction is z itself: the old p is never read then (it may be
+    // memory no solve has written yet, and 0 * NaN would poison every pass)
+    p[i] = first ? z[i] : z[i] + beta * p[i];
+    pt[i] = first ? zt[i] : zt[i] + beta * pt[i];
 }
 
 // (3) q = K p, q~ = K^T p~ (FP32), a warp per row; den = p~ . q (FP64)

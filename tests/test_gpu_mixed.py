@@ -165,3 +165,26 @@ def test_mixed_newton_loop_elastic_range(cuda_lib):
     u_err = float(np.abs(umx - u64).max() / np.abs(u64).max())
     print(f"elastic RVE, mixed vs FP64: stress {s_err:.2e}, u {u_err:.2e}")
     assert s_err < 1e-6 and u_err < 1e-6, (s_err, u_err)
+
+
+def test_mixed_inner_solve_ignores_stale_device_memory(cuda_lib):
+    """The FP32 inner solve's vectors are allocated on a handle's first mixed
+    Newton step.  Nothing that memory held before may reach the solve: the
+    vectors start as zeros and the first direction of every pass is z itself
+    (0 * NaN would otherwise turn every FP32 pass into NaN and hand the whole
+    run to the FP64 fallback).  Device memory filled with NaN is released just
+    before the handle is made, so that stale values are likely (not certain)
+    to land in its buffers; on the elastic 8^3 RVE every Newton step must then
+    converge with FP32 passes alone."""
+    import torch
+    junk = torch.full((1 << 30,), float("nan"), dtype=torch.float32, device="cuda")  # 4 GB of NaN
+    torch.cuda.synchronize()
+    del junk
+    torch.cuda.empty_cache()
+    mesh = H.StructuredMesh((8, 8, 8))
+    rod = np.repeat(M.random_rodrigues(np.random.default_rng(0), mesh.n_cells), 8, axis=0)
+    be, h = _rve_handle(mesh, rod, RVE_BC, CP_PRECISION_MIXED, 3, total_strain=2e-4)
+    info = h.solve_info
+    assert info and all(i["converged"] for i in info), info
+    assert all(i["fp64_iterations"] == 0 for i in info), [i["fp64_iterations"] for i in info]
+    be.close()
