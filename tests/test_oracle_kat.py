@@ -85,3 +85,27 @@ def test_golden_curve_cyclic_full(oracle_lib):
     assert err["strain"] < 1e-2 and err["slip"] < 1e-2, err
     assert H.golden_errors(rows, d["golden"], 400)["stress"] < 1e-2
     assert err["stress"] < 5e-2, err
+
+
+@pytest.mark.slow
+def test_cyclic_stress_beyond_row_400_is_set_by_rounding(oracle_lib):
+    """Why the cyclic deck's stress is bounded only over its first 400 rows:
+    the oracle as written and the oracle compiled with fused multiply-adds
+    (two equally valid roundings of the same arithmetic) stay within the
+    reference's 1e-2 of each other in von Mises stress over the first 400 rows
+    (measured 1.4e-3 over the first 100, 4.0e-3 over 400) and part by more
+    than that beyond (3.0e-2 at row 587): the same size as every
+    implementation's distance from the golden curve there."""
+    rows_a, _ = _run(oracle_lib, "fcc_CyclicLoading", 999)
+    prev = oracle_lib.use_library(oracle_lib.build_fma())
+    try:
+        rows_b, _ = _run(oracle_lib, "fcc_CyclicLoading", 999)
+    finally:
+        oracle_lib.restore_library(prev)
+    _, sa = H.von_mises_rows(rows_a)
+    _, sb = H.von_mises_rows(rows_b)
+    rel = np.abs(sa - sb) / np.abs(sa)
+    print(f"cyclic deck, oracle vs its FMA build: von Mises stress {rel[:100].max():.1e} over rows < 100, "
+          f"{rel[:400].max():.1e} over rows < 400, {rel[400:].max():.1e} beyond (row {400 + int(rel[400:].argmax())})")
+    assert rel[:400].max() < 1e-2
+    assert rel[400:].max() > 1e-2
